@@ -1,0 +1,234 @@
+"""carpetx_b200: B200 (sm_100a) refinement-factor-2 transfer operators of CarpetX.
+
+Python bindings over the C ABI of ``include/carpetx_b200.h`` (ctypes), used by
+the tests, the benchmark and the autograd wrappers.  FABs are CUDA float64
+tensors of shape ``(ncomp, nz, ny, nx)`` (x fastest, component stride = box
+points: the amrex::FArrayBox layout); boxes are inclusive ``(lo, hi)`` integer
+triples in AMReX index space.
+
+The compiled library ``libcarpetx_b200.so`` must exist next to this file (build
+it with ``python -m carpetx_b200.build``); there is no CPU fallback: every
+call raises if the library or a CUDA device is missing.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcarpetx_b200.so")
+
+# status codes (include/carpetx_b200.h)
+CX_OK, CX_EINVAL, CX_EUNSUPPORTED, CX_ECUDA, CX_ETIMEOUT, CX_ENOMEM, CX_ENODEVICE = range(7)
+
+FAMILIES = {
+    # prolongation_type -> orders (CarpetX/src/prolongate_3d_rf2_impl_*.cxx)
+    "interpolate": (1, 3, 5, 7),
+    "conservative": (0, 1),
+    "ddf": (1, 3, 5, 7),
+    "eno": (3, 5),
+    "minmod": (1, 3, 5),
+    "hermite": (1, 3, 5),
+    "natural": (1, 3, 5, 7),
+    "poly-cons3lfb": (1, 3, 5),
+    "poly-eno3lfb": (1, 3, 5),
+}
+
+
+class CxError(RuntimeError):
+    """A non-zero status from the C ABI."""
+
+    def __init__(self, status, message):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+_I3 = ctypes.c_int * 3
+_VP = ctypes.c_void_p
+_I = ctypes.c_int
+_lib = None
+
+
+class CxBox(ctypes.Structure):
+    """cx_box_t"""
+    _fields_ = [("op", ctypes.c_int32), ("ncomp", _I), ("crse", _VP), ("crse_lo", _I3),
+                ("crse_hi", _I3), ("fine", _VP), ("fine_lo", _I3), ("fine_hi", _I3),
+                ("reg_lo", _I3), ("reg_hi", _I3)]
+
+
+def lib():
+    """The loaded C library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: run python -m carpetx_b200.build")
+        L = ctypes.CDLL(LIB_PATH)
+        L.cx_status_string.restype = ctypes.c_char_p
+        L.cx_status_string.argtypes = [_I]
+        L.cx_last_error.restype = ctypes.c_char_p
+        L.cx_prolong_lookup.argtypes = [ctypes.c_char_p, _I, _I, ctypes.POINTER(ctypes.c_int32)]
+        L.cx_prolong_required_ghosts.argtypes = [ctypes.c_int32, _I3]
+        L.cx_prolong_coarse_box.argtypes = [ctypes.c_int32, _I3, _I3, _I3, _I3]
+        L.cx_prolong_box.argtypes = [ctypes.c_int32, _VP, _I3, _I3, _VP, _I3, _I3, _I3, _I3, _I, _I,
+                                     _VP]
+        L.cx_prolong_box_diag.argtypes = [ctypes.c_int32, _VP, _I3, _I3, _VP, _I3, _I3, _I3, _I3,
+                                          _I, _I, _VP, _VP, _VP]
+        L.cx_level_plan_create.argtypes = [ctypes.POINTER(CxBox), _I, _I, ctypes.POINTER(_VP)]
+        L.cx_level_plan_execute.argtypes = [_VP, _VP]
+        L.cx_level_plan_stats.argtypes = [_VP, ctypes.POINTER(ctypes.c_int64),
+                                          ctypes.POINTER(ctypes.c_int64),
+                                          ctypes.POINTER(ctypes.c_int64)]
+        L.cx_level_plan_destroy.argtypes = [_VP]
+        L.cx_restrict_box.argtypes = [_I, _VP, _I3, _I3, _VP, _I3, _I3, _I3, _I3, _I, _VP]
+        L.cx_restrict_adjoint_box.argtypes = [_I, _VP, _I3, _I3, _VP, _I3, _I3, _I3, _I3, _I, _VP]
+        L.cx_prolong_adjoint_box.argtypes = [ctypes.c_int32, _VP, _I3, _I3, _VP, _I3, _I3, _I3,
+                                             _I3, _I, _I, _VP, _VP]
+        _lib = L
+    return _lib
+
+
+def _check(status):
+    if status != CX_OK:
+        L = lib()
+        raise CxError(status, f"{L.cx_status_string(status).decode()}: "
+                              f"{L.cx_last_error().decode()}")
+
+
+def _i3(v):
+    return _I3(*[int(x) for x in v])
+
+
+def box_shape(lo, hi):
+    """(nz, ny, nx) of the inclusive box [lo, hi]."""
+    return tuple(int(hi[d]) - int(lo[d]) + 1 for d in (2, 1, 0))
+
+
+def _stream(stream):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+def _ptr(t, ncomp, lo, hi, what):
+    import torch
+    if not isinstance(t, torch.Tensor) or t.dtype != torch.float64 or not t.is_cuda:
+        raise TypeError(f"{what} must be a CUDA float64 tensor")
+    if not t.is_contiguous() or t.numel() < ncomp * _npts(lo, hi):
+        raise ValueError(f"{what} must be contiguous with ncomp x box points elements")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _npts(lo, hi):
+    n = 1
+    for a, b in zip(lo, hi):
+        n *= max(0, int(b) - int(a) + 1)
+    return n
+
+
+class Op:
+    """A prolongation operator: (prolongation_type, order, indextype)."""
+
+    def __init__(self, typ, order, indextype):
+        h = ctypes.c_int32()
+        _check(lib().cx_prolong_lookup(typ.encode(), int(order), int(indextype), ctypes.byref(h)))
+        self.handle = h.value
+        self.type, self.order, self.indextype = typ, int(order), int(indextype)
+
+    def required_ghosts(self):
+        g = _I3()
+        _check(lib().cx_prolong_required_ghosts(self.handle, g))
+        return tuple(g)
+
+    def coarse_box(self, fine_lo, fine_hi):
+        lo, hi = _I3(), _I3()
+        _check(lib().cx_prolong_coarse_box(self.handle, _i3(fine_lo), _i3(fine_hi), lo, hi))
+        return tuple(lo), tuple(hi)
+
+    def __repr__(self):
+        return f"Op({self.type!r}, {self.order}, {self.indextype})"
+
+
+def prolong_box(op, crse, crse_lo, crse_hi, fine, fine_lo, fine_hi, reg_lo, reg_hi, ncomp,
+                per_group=False, stream=None, shifts=None, fallback=None):
+    """cx_prolong_box / cx_prolong_box_diag on CUDA tensors (asynchronous)."""
+    L = lib()
+    args = (op.handle, _ptr(crse, ncomp, crse_lo, crse_hi, "crse"), _i3(crse_lo), _i3(crse_hi),
+            _ptr(fine, ncomp, fine_lo, fine_hi, "fine"), _i3(fine_lo), _i3(fine_hi), _i3(reg_lo),
+            _i3(reg_hi), int(ncomp), int(bool(per_group)))
+    if shifts is None and fallback is None:
+        _check(L.cx_prolong_box(*args, _stream(stream)))
+    else:
+        _check(L.cx_prolong_box_diag(
+            *args, ctypes.c_void_p(shifts.data_ptr() if shifts is not None else 0),
+            ctypes.c_void_p(fallback.data_ptr() if fallback is not None else 0), _stream(stream)))
+
+
+def restrict_box(indextype, fine, fine_lo, fine_hi, crse, crse_lo, crse_hi, reg_lo, reg_hi, ncomp,
+                 stream=None):
+    """cx_restrict_box on CUDA tensors (asynchronous)."""
+    _check(lib().cx_restrict_box(int(indextype), _ptr(fine, ncomp, fine_lo, fine_hi, "fine"),
+                                 _i3(fine_lo), _i3(fine_hi),
+                                 _ptr(crse, ncomp, crse_lo, crse_hi, "crse"), _i3(crse_lo),
+                                 _i3(crse_hi), _i3(reg_lo), _i3(reg_hi), int(ncomp),
+                                 _stream(stream)))
+
+
+def prolong_adjoint_box(op, crse, crse_lo, crse_hi, fine_bar, fine_lo, fine_hi, reg_lo, reg_hi,
+                        ncomp, crse_bar, per_group=False, stream=None):
+    """cx_prolong_adjoint_box: crse_bar = P^T fine_bar (asynchronous)."""
+    _check(lib().cx_prolong_adjoint_box(
+        op.handle, _ptr(crse, ncomp, crse_lo, crse_hi, "crse"), _i3(crse_lo), _i3(crse_hi),
+        _ptr(fine_bar, ncomp, fine_lo, fine_hi, "fine_bar"), _i3(fine_lo), _i3(fine_hi),
+        _i3(reg_lo), _i3(reg_hi), int(ncomp), int(bool(per_group)),
+        _ptr(crse_bar, ncomp, crse_lo, crse_hi, "crse_bar"), _stream(stream)))
+
+
+def restrict_adjoint_box(indextype, crse_bar, crse_lo, crse_hi, fine_bar, fine_lo, fine_hi,
+                         reg_lo, reg_hi, ncomp, stream=None):
+    """cx_restrict_adjoint_box: fine_bar = R^T crse_bar (asynchronous)."""
+    _check(lib().cx_restrict_adjoint_box(
+        int(indextype), _ptr(crse_bar, ncomp, crse_lo, crse_hi, "crse_bar"), _i3(crse_lo),
+        _i3(crse_hi), _ptr(fine_bar, ncomp, fine_lo, fine_hi, "fine_bar"), _i3(fine_lo),
+        _i3(fine_hi), _i3(reg_lo), _i3(reg_hi), int(ncomp), _stream(stream)))
+
+
+class LevelPlan:
+    """cx_level_plan_*: a whole level transfer as one persistent launch.
+
+    boxes: iterable of dicts with keys op, ncomp, crse, crse_lo, crse_hi, fine,
+    fine_lo, fine_hi, reg_lo, reg_hi (tensors as for prolong_box).  The plan
+    keeps references to the tensors so their memory outlives it."""
+
+    def __init__(self, boxes, per_group=False):
+        self._keep = []
+        arr = (CxBox * max(1, len(boxes)))()
+        for i, b in enumerate(boxes):
+            n = int(b["ncomp"])
+            arr[i] = CxBox(b["op"].handle, n,
+                           _ptr(b["crse"], n, b["crse_lo"], b["crse_hi"], "crse").value,
+                           _i3(b["crse_lo"]), _i3(b["crse_hi"]),
+                           _ptr(b["fine"], n, b["fine_lo"], b["fine_hi"], "fine").value,
+                           _i3(b["fine_lo"]), _i3(b["fine_hi"]), _i3(b["reg_lo"]),
+                           _i3(b["reg_hi"]))
+            self._keep += [b["crse"], b["fine"]]
+        h = ctypes.c_void_p()
+        _check(lib().cx_level_plan_create(arr, len(boxes), int(bool(per_group)), ctypes.byref(h)))
+        self.handle = h
+
+    def execute(self, stream=None):
+        _check(lib().cx_level_plan_execute(self.handle, _stream(stream)))
+
+    def stats(self):
+        a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().cx_level_plan_stats(self.handle, ctypes.byref(a), ctypes.byref(b),
+                                         ctypes.byref(c)))
+        return {"tiles": a.value, "fine_points": b.value, "bytes": c.value}
+
+    def close(self):
+        if self.handle:
+            lib().cx_level_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

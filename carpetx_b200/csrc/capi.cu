@@ -1,0 +1,499 @@
+// The C ABI (include/carpetx_b200.h): operator registry, argument
+// validation, dispatch to the kernels, level plans.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/carpetx_b200.h"
+#include "cx_internal.h"
+
+using namespace cxb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int status, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return status;
+}
+
+int cuda_status(cudaError_t e, const char *what) {
+  if (e == cudaSuccess)
+    return CX_OK;
+  return fail(CX_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// Kinds of a family for one direction (the nine tables of
+// CarpetX/src/prolongate_3d_rf2_impl_*.cxx).
+int vc_poly_kind(int p) {
+  return p == 1 ? K_VC_POLY1 : p == 3 ? K_VC_POLY3 : p == 5 ? K_VC_POLY5 : p == 7 ? K_VC_POLY7 : -1;
+}
+int cc_poly_kind(int p) {
+  return p == 1 ? K_CC_POLY1 : p == 3 ? K_CC_POLY3 : p == 5 ? K_CC_POLY5 : p == 7 ? K_CC_POLY7 : -1;
+}
+int cc_cons_kind(int p) { return p >= 0 && p <= 7 ? K_CC_CONS0 + p : -1; }
+
+bool lookup_kinds(const char *type, int o, int *vc, int *cc, int *fb) {
+  const std::string t(type);
+  *fb = 0;
+  auto in = [o](std::initializer_list<int> l) { return std::find(l.begin(), l.end(), o) != l.end(); };
+  if (t == "interpolate" && in({1, 3, 5, 7})) { // impl_poly.cxx:7-121
+    *vc = vc_poly_kind(o);
+    *cc = cc_poly_kind(o);
+  } else if (t == "conservative" && in({0, 1})) { // impl_cons.cxx:7-65
+    *vc = o == 0 ? K_VC_CONS0 : K_VC_CONS1;
+    *cc = o == 0 ? K_CC_CONS0 : K_CC_CONS2;
+  } else if (t == "ddf" && in({1, 3, 5, 7})) { // impl_ddf.cxx:7-121
+    *vc = vc_poly_kind(o);
+    *cc = cc_cons_kind(o - 1);
+  } else if (t == "eno" && in({3, 5})) { // impl_eno.cxx:7-65
+    *vc = vc_poly_kind(o);
+    *cc = K_CC_ENO2;
+  } else if (t == "minmod" && in({1, 3, 5})) { // impl_minmod.cxx:7-93
+    *vc = vc_poly_kind(o);
+    *cc = K_CC_MINMOD1;
+  } else if ((t == "hermite" && in({1, 3, 5})) || (t == "natural" && in({1, 3, 5, 7}))) {
+    // impl_hermite.cxx:7-96 (VC HERMITE = VC POLY arithmetic), impl_natural.cxx:7-121
+    *vc = vc_poly_kind(o);
+    *cc = cc_cons_kind(o);
+  } else if (t == "poly-cons3lfb" && in({1, 3, 5})) { // impl_poly_cons3lfb.cxx:9-119
+    *vc = vc_poly_kind(o);
+    *cc = cc_cons_kind(std::min(o, 3));
+    *fb = 1;
+  } else if (t == "poly-eno3lfb" && in({1, 3, 5})) { // impl_poly_eno3lfb.cxx:9-119
+    *vc = vc_poly_kind(o);
+    *cc = o == 1 ? K_CC_CONS0 : K_CC_ENO2;
+    *fb = 1;
+  } else {
+    return false;
+  }
+  return true;
+}
+
+bool valid_op(cx_op_t op) {
+  for (int d = 0; d < 3; ++d)
+    if (op_kind(op, d) < 0 || op_kind(op, d) >= K_COUNT)
+      return false;
+  return (op >> 16) == 0;
+}
+
+int floor2(int i) { return i >= 0 ? i / 2 : -((-i + 1) / 2); }
+
+bool box_ok(const int lo[3], const int hi[3]) {
+  return lo[0] <= hi[0] && lo[1] <= hi[1] && lo[2] <= hi[2];
+}
+
+// Builds and validates the kernel descriptor of one interp() call.
+// Returns CX_OK, or an error; *empty is set when there is nothing to do.
+int make_box(cx_op_t op, const double *crse, const int clo[3], const int chi[3], double *fine,
+             const int flo[3], const int fhi[3], const int rlo[3], const int rhi[3], int ncomp,
+             int per_group, BoxDesc *b, bool *empty) {
+  *empty = false;
+  if (!valid_op(op))
+    return fail(CX_EUNSUPPORTED, "invalid operator handle %d", (int)op);
+  if (!clo || !chi || !flo || !fhi || !rlo || !rhi)
+    return fail(CX_EINVAL, "null box pointer");
+  if (ncomp < 0)
+    return fail(CX_EINVAL, "ncomp = %d < 0", ncomp);
+  if (per_group && ncomp > 16) // impl.hxx:1707-1708
+    return fail(CX_EINVAL, "per-group prolongation supports at most 16 components, got %d", ncomp);
+  if (!box_ok(rlo, rhi) || ncomp == 0) {
+    *empty = true;
+    return CX_OK;
+  }
+  if (!crse || !fine)
+    return fail(CX_EINVAL, "null data pointer");
+  if (!box_ok(flo, fhi) || !box_ok(clo, chi))
+    return fail(CX_EINVAL, "empty coarse or fine FAB box");
+  for (int d = 0; d < 3; ++d)
+    if (rlo[d] < flo[d] || rhi[d] > fhi[d]) // impl.hxx:1300-1302
+      return fail(CX_EINVAL, "fine region [%d,%d] not inside the fine box [%d,%d] in direction %d",
+                  rlo[d], rhi[d], flo[d], fhi[d], d);
+  std::memset(b, 0, sizeof *b);
+  b->crse = crse;
+  b->fine = fine;
+  b->op = op;
+  b->ncomp = ncomp;
+  const int T[3] = {kSepTX, kSepTY, kSepTZ};
+  for (int d = 0; d < 3; ++d) {
+    const int k = op_kind(op, d);
+    b->kind[d] = k;
+    b->clo[d] = clo[d];
+    b->flo[d] = flo[d];
+    b->rlo[d] = rlo[d];
+    b->rhi[d] = rhi[d];
+    // coarse points read: extreme fine points of each parity
+    int nlo = INT32_MAX, nhi = INT32_MIN;
+    for (int f = rlo[d]; f <= rhi[d] && f <= rlo[d] + 1; ++f) {
+      int a, c;
+      read_range(k, f & 1, &a, &c);
+      nlo = std::min(nlo, floor2(f) + a);
+    }
+    for (int f = rhi[d]; f >= rlo[d] && f >= rhi[d] - 1; --f) {
+      int a, c;
+      read_range(k, f & 1, &a, &c);
+      nhi = std::max(nhi, floor2(f) + c);
+    }
+    if (nlo < clo[d] || nhi > chi[d])
+      return fail(CX_EINVAL,
+                  "coarse box [%d,%d] does not contain the coarse points [%d,%d] the stencil "
+                  "reads in direction %d",
+                  clo[d], chi[d], nlo, nhi, d);
+    b->nlo[d] = nlo;
+    b->nhi[d] = nhi;
+    b->tbase[d] = rlo[d] & ~1;
+    b->ntile[d] = (rhi[d] - b->tbase[d] + T[d]) / T[d];
+  }
+  b->cnx = chi[0] - clo[0] + 1;
+  b->cny = chi[1] - clo[1] + 1;
+  b->cnp = (int64_t)b->cnx * b->cny * (chi[2] - clo[2] + 1);
+  b->fnx = fhi[0] - flo[0] + 1;
+  b->fny = fhi[1] - flo[1] + 1;
+  b->fnp = (int64_t)b->fnx * b->fny * (fhi[2] - flo[2] + 1);
+  (void)per_group;
+  return CX_OK;
+}
+
+int check_device() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(CX_ENODEVICE, "no CUDA device");
+  }
+  return CX_OK;
+}
+
+int64_t box_points(const int lo[3], const int hi[3]) {
+  return (int64_t)(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+}
+
+} // namespace
+
+struct cx_level_plan {
+  int per_group = 0;
+  std::vector<BoxDesc> boxes;
+  std::vector<int> point_boxes; // boxes handled by the pointwise kernel
+  BoxDesc *d_boxes = nullptr;
+  TileRef *d_tiles = nullptr;
+  int *d_counter = nullptr;
+  int nsep_tiles = 0;
+  int s0max = 0, s1max = 0;
+  size_t smem = 0;
+  int grid = 0;
+  int64_t nfine = 0, bytes = 0;
+};
+
+extern "C" {
+
+const char *cx_status_string(int status) {
+  switch (status) {
+  case CX_OK: return "ok";
+  case CX_EINVAL: return "invalid argument";
+  case CX_EUNSUPPORTED: return "unsupported operator";
+  case CX_ECUDA: return "CUDA error";
+  case CX_ETIMEOUT: return "device wait timed out";
+  case CX_ENOMEM: return "out of memory";
+  case CX_ENODEVICE: return "no CUDA device";
+  default: return "unknown status";
+  }
+}
+
+const char *cx_last_error(void) { return g_last_error.c_str(); }
+
+int cx_prolong_lookup(const char *type, int order, int indextype, cx_op_t *out) {
+  if (!type || !out)
+    return fail(CX_EINVAL, "null argument");
+  if (indextype < 0 || indextype > 7)
+    return fail(CX_EUNSUPPORTED, "indextype %d out of range 0..7", indextype);
+  int vc, cc, fb;
+  if (!lookup_kinds(type, order, &vc, &cc, &fb))
+    return fail(CX_EUNSUPPORTED, "Unsupported prolongation order %d for prolongation type %s",
+                order, type);
+  int k[3];
+  for (int d = 0; d < 3; ++d)
+    k[d] = ((indextype >> (2 - d)) & 1) ? cc : vc;
+  *out = op_encode(k[0], k[1], k[2], fb);
+  return CX_OK;
+}
+
+int cx_prolong_required_ghosts(cx_op_t op, int ghosts[3]) {
+  if (!valid_op(op) || !ghosts)
+    return fail(CX_EINVAL, "invalid argument");
+  for (int d = 0; d < 3; ++d)
+    ghosts[d] = kind_info(op_kind(op, d)).ghosts;
+  return CX_OK;
+}
+
+int cx_prolong_coarse_box(cx_op_t op, const int fine_lo[3], const int fine_hi[3], int crse_lo[3],
+                          int crse_hi[3]) {
+  int g[3];
+  if (!fine_lo || !fine_hi || !crse_lo || !crse_hi)
+    return fail(CX_EINVAL, "null argument");
+  if (int e = cx_prolong_required_ghosts(op, g))
+    return e;
+  for (int d = 0; d < 3; ++d) {
+    crse_lo[d] = floor2(fine_lo[d]) - g[d];
+    crse_hi[d] = floor2(fine_hi[d]) + g[d];
+  }
+  return CX_OK;
+}
+
+int cx_prolong_box_diag(cx_op_t op, const double *crse, const int crse_lo[3], const int crse_hi[3],
+                        double *fine, const int fine_lo[3], const int fine_hi[3],
+                        const int reg_lo[3], const int reg_hi[3], int ncomp, int per_group,
+                        signed char *shifts, unsigned char *fallback, cx_stream_t stream) {
+  BoxDesc b;
+  bool empty;
+  if (int e = make_box(op, crse, crse_lo, crse_hi, fine, fine_lo, fine_hi, reg_lo, reg_hi, ncomp,
+                       per_group, &b, &empty))
+    return e;
+  if (empty)
+    return CX_OK;
+  if (int e = check_device())
+    return e;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (op_separable(op, per_group) && !shifts && !fallback)
+    return cuda_status(launch_sep_box(b, s), "prolongation launch");
+  if (op_separable(op, per_group)) {
+    // diagnostics requested for an operator without shifts or fallback:
+    // values from the separable kernel, diagnostics all zero
+    const int64_t nreg = box_points(reg_lo, reg_hi) * (per_group ? 1 : ncomp);
+    if (shifts)
+      if (int e = cuda_status(cudaMemsetAsync(shifts, 0, 3 * nreg, s), "memset"))
+        return e;
+    if (fallback)
+      if (int e = cuda_status(cudaMemsetAsync(fallback, 0, nreg, s), "memset"))
+        return e;
+    return cuda_status(launch_sep_box(b, s), "prolongation launch");
+  }
+  return cuda_status(launch_point_box(b, per_group, shifts, fallback, s), "prolongation launch");
+}
+
+int cx_prolong_box(cx_op_t op, const double *crse, const int crse_lo[3], const int crse_hi[3],
+                   double *fine, const int fine_lo[3], const int fine_hi[3], const int reg_lo[3],
+                   const int reg_hi[3], int ncomp, int per_group, cx_stream_t stream) {
+  return cx_prolong_box_diag(op, crse, crse_lo, crse_hi, fine, fine_lo, fine_hi, reg_lo, reg_hi,
+                             ncomp, per_group, nullptr, nullptr, stream);
+}
+
+int cx_level_plan_create(const cx_box_t *boxes, int nboxes, int per_group, cx_level_plan_t *out) {
+  if (!out || nboxes < 0 || (nboxes > 0 && !boxes))
+    return fail(CX_EINVAL, "invalid argument");
+  *out = nullptr;
+  if (int e = check_device())
+    return e;
+  cx_level_plan *p = new cx_level_plan;
+  p->per_group = per_group;
+  std::vector<int> sep_ids;
+  for (int i = 0; i < nboxes; ++i) {
+    const cx_box_t &x = boxes[i];
+    BoxDesc b;
+    bool empty;
+    if (int e = make_box(x.op, x.crse, x.crse_lo, x.crse_hi, x.fine, x.fine_lo, x.fine_hi,
+                         x.reg_lo, x.reg_hi, x.ncomp, per_group, &b, &empty)) {
+      delete p;
+      return fail(e, "box %d: %s", i, g_last_error.c_str());
+    }
+    if (empty)
+      continue;
+    int g[3], cl[3], ch[3];
+    cx_prolong_coarse_box(x.op, x.reg_lo, x.reg_hi, cl, ch);
+    (void)g;
+    p->nfine += box_points(x.reg_lo, x.reg_hi) * x.ncomp;
+    p->bytes += 8 * (box_points(cl, ch) + box_points(x.reg_lo, x.reg_hi)) * x.ncomp;
+    const int id = (int)p->boxes.size();
+    p->boxes.push_back(b);
+    if (op_separable(x.op, per_group))
+      sep_ids.push_back(id);
+    else
+      p->point_boxes.push_back(id);
+  }
+  // tiles of the separable boxes, largest boxes first (longest-processing-
+  // time order for the dynamic scheduler), x fastest within a box
+  std::sort(sep_ids.begin(), sep_ids.end(), [&](int a, int b) {
+    const BoxDesc &A = p->boxes[a], &B = p->boxes[b];
+    const int64_t na = (int64_t)A.ntile[0] * A.ntile[1] * A.ntile[2];
+    const int64_t nb = (int64_t)B.ntile[0] * B.ntile[1] * B.ntile[2];
+    return na != nb ? na > nb : a < b;
+  });
+  std::vector<TileRef> tiles;
+  for (int id : sep_ids) {
+    const BoxDesc &b = p->boxes[id];
+    const SepSmem m = sep_smem_for(b.kind);
+    p->s0max = std::max(p->s0max, m.s0);
+    p->s1max = std::max(p->s1max, m.s1);
+    p->smem = std::max(p->smem, (size_t)0);
+    for (int c = 0; c < b.ncomp; ++c)
+      for (int tz = 0; tz < b.ntile[2]; ++tz)
+        for (int ty = 0; ty < b.ntile[1]; ++ty)
+          for (int tx = 0; tx < b.ntile[0]; ++tx)
+            tiles.push_back(TileRef{id, (int16_t)tx, (int16_t)ty, (int16_t)tz, (int16_t)c});
+  }
+  int s2max = 0;
+  for (int id : sep_ids)
+    s2max = std::max(s2max, sep_smem_for(p->boxes[id].kind).s2);
+  p->smem = sizeof(double) * (size_t)(2 * p->s0max + p->s1max + s2max);
+  if (tiles.size() > (size_t)INT32_MAX) {
+    delete p;
+    return fail(CX_EINVAL, "too many tiles");
+  }
+  p->nsep_tiles = (int)tiles.size();
+  cudaError_t e = cudaSuccess;
+  if (!p->boxes.empty())
+    e = cudaMalloc(&p->d_boxes, sizeof(BoxDesc) * p->boxes.size());
+  if (e == cudaSuccess && !tiles.empty())
+    e = cudaMalloc(&p->d_tiles, sizeof(TileRef) * tiles.size());
+  if (e == cudaSuccess)
+    e = cudaMalloc(&p->d_counter, sizeof(int));
+  if (e == cudaSuccess && !p->boxes.empty())
+    e = cudaMemcpy(p->d_boxes, p->boxes.data(), sizeof(BoxDesc) * p->boxes.size(),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !tiles.empty())
+    e = cudaMemcpy(p->d_tiles, tiles.data(), sizeof(TileRef) * tiles.size(),
+                   cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cx_level_plan_destroy(p);
+    return fail(e == cudaErrorMemoryAllocation ? CX_ENOMEM : CX_ECUDA, "level plan: %s",
+                cudaGetErrorString(e));
+  }
+  p->grid = p->nsep_tiles ? sep_level_grid(p->smem) : 0;
+  *out = p;
+  return CX_OK;
+}
+
+int cx_level_plan_execute(cx_level_plan_t p, cx_stream_t stream) {
+  if (!p)
+    return fail(CX_EINVAL, "null plan");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (p->nsep_tiles)
+    if (int e = cuda_status(launch_sep_level(p->d_boxes, p->d_tiles, p->nsep_tiles, p->d_counter,
+                                             p->s0max, p->s1max, p->smem, p->grid, s),
+                            "level launch"))
+      return e;
+  for (int id : p->point_boxes)
+    if (int e = cuda_status(launch_point_box(p->boxes[id], p->per_group, nullptr, nullptr, s),
+                            "level launch (limited operators)"))
+      return e;
+  return CX_OK;
+}
+
+int cx_level_plan_stats(cx_level_plan_t p, int64_t *ntiles, int64_t *nfine, int64_t *bytes) {
+  if (!p)
+    return fail(CX_EINVAL, "null plan");
+  if (ntiles)
+    *ntiles = p->nsep_tiles;
+  if (nfine)
+    *nfine = p->nfine;
+  if (bytes)
+    *bytes = p->bytes;
+  return CX_OK;
+}
+
+int cx_level_plan_destroy(cx_level_plan_t p) {
+  if (!p)
+    return CX_OK;
+  cudaFree(p->d_boxes);
+  cudaFree(p->d_tiles);
+  cudaFree(p->d_counter);
+  delete p;
+  return CX_OK;
+}
+
+int cx_restrict_box(int indextype, const double *fine, const int fine_lo[3], const int fine_hi[3],
+                    double *crse, const int crse_lo[3], const int crse_hi[3], const int reg_lo[3],
+                    const int reg_hi[3], int ncomp, cx_stream_t stream) {
+  if (indextype < 0 || indextype > 7)
+    return fail(CX_EUNSUPPORTED, "indextype %d out of range 0..7", indextype);
+  if (!fine_lo || !fine_hi || !crse_lo || !crse_hi || !reg_lo || !reg_hi || ncomp < 0)
+    return fail(CX_EINVAL, "invalid argument");
+  if (!box_ok(reg_lo, reg_hi) || ncomp == 0)
+    return CX_OK;
+  if (!fine || !crse || !box_ok(fine_lo, fine_hi) || !box_ok(crse_lo, crse_hi))
+    return fail(CX_EINVAL, "invalid FAB");
+  for (int d = 0; d < 3; ++d) {
+    const int cc = (indextype >> (2 - d)) & 1;
+    if (reg_lo[d] < crse_lo[d] || reg_hi[d] > crse_hi[d])
+      return fail(CX_EINVAL, "coarse region not inside the coarse box in direction %d", d);
+    if (2 * reg_lo[d] < fine_lo[d] || 2 * reg_hi[d] + cc > fine_hi[d])
+      return fail(CX_EINVAL, "fine box does not contain the children of the region in direction %d",
+                  d);
+  }
+  if (int e = check_device())
+    return e;
+  return cuda_status(launch_restrict_box(indextype, fine, fine_lo, fine_hi, crse, crse_lo, crse_hi,
+                                         reg_lo, reg_hi, ncomp, (cudaStream_t)stream),
+                     "restriction launch");
+}
+
+int cx_restrict_adjoint_box(int indextype, const double *crse_bar, const int crse_lo[3],
+                            const int crse_hi[3], double *fine_bar, const int fine_lo[3],
+                            const int fine_hi[3], const int reg_lo[3], const int reg_hi[3],
+                            int ncomp, cx_stream_t stream) {
+  if (indextype < 0 || indextype > 7)
+    return fail(CX_EUNSUPPORTED, "indextype %d out of range 0..7", indextype);
+  if (!fine_lo || !fine_hi || !crse_lo || !crse_hi || !reg_lo || !reg_hi || ncomp < 0)
+    return fail(CX_EINVAL, "invalid argument");
+  if (!fine_bar || !crse_bar || !box_ok(fine_lo, fine_hi) || !box_ok(crse_lo, crse_hi))
+    return fail(CX_EINVAL, "invalid FAB");
+  if (box_ok(reg_lo, reg_hi))
+    for (int d = 0; d < 3; ++d) {
+      const int cc = (indextype >> (2 - d)) & 1;
+      if (reg_lo[d] < crse_lo[d] || reg_hi[d] > crse_hi[d] || 2 * reg_lo[d] < fine_lo[d] ||
+          2 * reg_hi[d] + cc > fine_hi[d])
+        return fail(CX_EINVAL, "region does not fit the boxes in direction %d", d);
+    }
+  if (int e = check_device())
+    return e;
+  int rlo[3], rhi[3];
+  for (int d = 0; d < 3; ++d) {
+    rlo[d] = reg_lo[d];
+    rhi[d] = reg_hi[d];
+  }
+  if (!box_ok(reg_lo, reg_hi)) // nothing restricted: the transpose is zero
+    rhi[0] = rlo[0] - 1;
+  return cuda_status(launch_restrict_adjoint_box(indextype, crse_bar, crse_lo, crse_hi, fine_bar,
+                                                 fine_lo, fine_hi, rlo, rhi, ncomp,
+                                                 (cudaStream_t)stream),
+                     "restriction adjoint launch");
+}
+
+int cx_prolong_adjoint_box(cx_op_t op, const double *crse, const int crse_lo[3],
+                           const int crse_hi[3], const double *fine_bar, const int fine_lo[3],
+                           const int fine_hi[3], const int reg_lo[3], const int reg_hi[3],
+                           int ncomp, int per_group, double *crse_bar, cx_stream_t stream) {
+  BoxDesc b;
+  bool empty;
+  if (!crse_bar)
+    return fail(CX_EINVAL, "null crse_bar");
+  if (int e = make_box(op, crse, crse_lo, crse_hi, const_cast<double *>(fine_bar), fine_lo, fine_hi,
+                       reg_lo, reg_hi, ncomp, per_group, &b, &empty))
+    return e;
+  if (int e = check_device())
+    return e;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (empty) {
+    if (ncomp > 0 && box_ok(crse_lo, crse_hi))
+      return cuda_status(
+          cudaMemsetAsync(crse_bar, 0, sizeof(double) * box_points(crse_lo, crse_hi) * ncomp, s),
+          "memset");
+    return CX_OK;
+  }
+  bool linear = op_separable(op, per_group);
+  for (int d = 0; d < 3; ++d)
+    linear = linear && b.kind[d] != K_CC_MINMOD1;
+  if (!linear)
+    return fail(CX_EUNSUPPORTED,
+                "adjoint of limited operators (ENO, minmod, linear fallback) is not available");
+  return cuda_status(launch_prolong_adjoint_box(b, per_group, crse_bar, s), "adjoint launch");
+}
+
+} // extern "C"

@@ -1,0 +1,259 @@
+// Pointwise prolongation kernel for the operators that are not separable:
+// ENO directions (stencil shift chosen per point from undivided differences)
+// and the FB_LINEAR fallback (poly-cons3lfb, poly-eno3lfb).
+//
+// One thread per fine point (per component in per-var mode), following the
+// reference loop body (CarpetX/src/prolongate_3d_rf2_impl.hxx:1412-1669 per
+// var, 1854-2146 per group) step by step: shift search, tensor evaluation,
+// fallback tests, store.  Coarse values are read through the read-only data
+// cache.  Stencil kinds are runtime parameters here.
+#include "cx_internal.h"
+#include "cx_stencils.cuh"
+
+namespace cxb {
+namespace {
+
+struct Coarse {
+  const double *p; // component 0
+  int64_t np;
+  int lo[3];
+  int nx, ny;
+  __device__ __forceinline__ double operator()(int comp, int i, int j, int k) const {
+    return __ldg(p + comp * np + (i - lo[0]) + (int64_t)nx * ((j - lo[1]) + (int64_t)ny * (k - lo[2])));
+  }
+};
+
+// stencil_radius(shift, off) of a kind (impl.hxx:402-408, 466-476, 588-601,
+// 640-649, 786-803, 850-856).
+__device__ __forceinline__ void radius(int k, int shift, int off, int r[2]) {
+  if (k == K_CC_ENO2) {
+    r[0] = shift - 1;
+    r[1] = shift + 1;
+    return;
+  }
+  const KindInfo ki = kind_info(k);
+  r[0] = off ? ki.r1lo : ki.r0lo;
+  r[1] = off ? ki.r1hi : ki.r0hi;
+}
+
+// interp1d<CC,ENO,2>: row m = shift + 1 (off 0) or 1 - shift (off 1), off 1
+// reverses the row (impl.hxx:806-841).
+__device__ __forceinline__ double eno2(int shift, int off, const double *v) {
+  const int m = off == 0 ? shift + 1 : 1 - shift;
+  const int i0 = 1 - shift;
+  double y = 0.0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    y = fadd(y, fmul(cc_eno2_c(m, off == 0 ? i : 2 - i), v[i - i0]));
+  return y;
+}
+
+template <class K> __device__ __forceinline__ void ap_off(int off, const double *v, double &y) {
+  y = off ? K::template ap<1>(v) : K::template ap<0>(v);
+}
+
+// Runtime-kind 1-D stencil; v points at coarse offset 0.
+__device__ __noinline__ double ap_rt(int k, int shift, int off, const double *v) {
+  if (k == K_CC_ENO2)
+    return eno2(shift, off, v);
+  double y = 0.0;
+  CXB_DISPATCH_SEPARABLE(k, ap_off, off, v, y);
+  return y;
+}
+
+// call_stencil_3d with runtime kinds (impl.hxx:1206-1216).
+__device__ double eval3d(const int kind[3], const int shift[3], const int off[3], const Coarse &c,
+                         int comp, const int ic[3]) {
+  int r[3][2];
+  for (int d = 0; d < 3; ++d)
+    radius(kind[d], shift[d], off[d], r[d]);
+  double Y[9], X[9], v[9];
+  for (int dk = r[2][0]; dk <= r[2][1]; ++dk) {
+    for (int dj = r[1][0]; dj <= r[1][1]; ++dj) {
+      for (int di = r[0][0]; di <= r[0][1]; ++di)
+        v[di + 4] = c(comp, ic[0] + di, ic[1] + dj, ic[2] + dk);
+      X[dj + 4] = ap_rt(kind[0], shift[0], off[0], v + 4);
+    }
+    Y[dk + 4] = ap_rt(kind[1], shift[1], off[1], X + 4);
+  }
+  return ap_rt(kind[2], shift[2], off[2], Y + 4);
+}
+
+// undivided_difference_1d<CC,ENO,2> (impl.hxx:751-773): -2*c0 + (c- + c+).
+__device__ __forceinline__ double undiv2(double cm, double c0, double cp) {
+  return fadd(fmul(-2.0, c0), fmul(1.0, fadd(cm, cp)));
+}
+
+// ENO shift choice (impl.hxx:1415-1517 / 1857-1965) over components c0..c1-1.
+__device__ void choose_shift(const int kind[3], const int off[3], const Coarse &c, int c0, int c1,
+                             const int ic[3], int shift[3]) {
+  int use[3], maxs[3];
+  for (int d = 0; d < 3; ++d) {
+    use[d] = kind[d] == K_CC_ENO2;
+    maxs[d] = use[d] ? 1 : 0;
+    shift[d] = 0;
+  }
+  double min_dd = __longlong_as_double(0x7ff0000000000000LL); // +inf
+  for (int sk = -maxs[2]; sk <= maxs[2]; ++sk)
+    for (int sj = -maxs[1]; sj <= maxs[1]; ++sj)
+      for (int si = -maxs[0]; si <= maxs[0]; ++si) {
+        const int sh[3] = {si, sj, sk};
+        int r[3][2];
+        for (int d = 0; d < 3; ++d) {
+          radius(kind[d], sh[d], off[d], r[d]);
+          if (use[d]) {
+            r[d][0] -= sh[d];
+            r[d][1] -= sh[d];
+          }
+        }
+        double ddx = 0, ddy = 0, ddz = 0;
+        for (int comp = c0; comp < c1; ++comp) {
+          if (use[0])
+            for (int dk = r[2][0]; dk <= r[2][1]; ++dk)
+              for (int dj = r[1][0]; dj <= r[1][1]; ++dj) {
+                const int i = ic[0] + si, j = ic[1] + sj + dj, k = ic[2] + sk + dk;
+                ddx = fmax(ddx, fabs(undiv2(c(comp, i - 1, j, k), c(comp, i, j, k), c(comp, i + 1, j, k))));
+              }
+          if (use[1])
+            for (int dk = r[2][0]; dk <= r[2][1]; ++dk)
+              for (int di = r[0][0]; di <= r[0][1]; ++di) {
+                const int i = ic[0] + si + di, j = ic[1] + sj, k = ic[2] + sk + dk;
+                ddy = fmax(ddy, fabs(undiv2(c(comp, i, j - 1, k), c(comp, i, j, k), c(comp, i, j + 1, k))));
+              }
+          if (use[2])
+            for (int dj = r[1][0]; dj <= r[1][1]; ++dj)
+              for (int di = r[0][0]; di <= r[0][1]; ++di) {
+                const int i = ic[0] + si + di, j = ic[1] + sj + dj, k = ic[2] + sk;
+                ddz = fmax(ddz, fabs(undiv2(c(comp, i, j, k - 1), c(comp, i, j, k), c(comp, i, j, k + 1))));
+              }
+        }
+        // 1 + sqrt(DBL_EPSILON) * n, sqrt(2^-52) = 2^-26 exactly
+        const double penalty = fadd(1.0, fmul(0x1p-26, (double)(abs(si) + abs(sj) + abs(sk))));
+        const double dd = fmul(penalty, fmax(fmax(ddx, ddy), ddz));
+        if (dd < min_dd) {
+          min_dd = dd;
+          shift[0] = si;
+          shift[1] = sj;
+          shift[2] = sk;
+        }
+      }
+}
+
+// Slope sign change in direction d (impl.hxx:1609-1664, 2026-2115): s0 is
+// taken between offsets 0 and 1, the scan starts at radius[0] + 2.
+__device__ bool slope_change(int d, const int sr[3][2], const Coarse &c, int comp, const int ic[3]) {
+  const int in_d = d == 0 ? 1 : 0, out_d = d == 2 ? 1 : 2;
+  bool need = false;
+  for (int q = sr[out_d][0]; q <= sr[out_d][1]; ++q)
+    for (int t = sr[in_d][0]; t <= sr[in_d][1]; ++t) {
+      int a[3], b[3];
+      a[out_d] = b[out_d] = q;
+      a[in_d] = b[in_d] = t;
+      a[d] = 1;
+      b[d] = 0;
+      const double s0 = fsub(c(comp, ic[0] + a[0], ic[1] + a[1], ic[2] + a[2]),
+                             c(comp, ic[0] + b[0], ic[1] + b[1], ic[2] + b[2]));
+      for (int e = sr[d][0] + 2; e <= sr[d][1]; ++e) {
+        a[d] = e;
+        b[d] = e - 1;
+        const double s = fsub(c(comp, ic[0] + a[0], ic[1] + a[1], ic[2] + a[2]),
+                              c(comp, ic[0] + b[0], ic[1] + b[1], ic[2] + b[2]));
+        need |= fmul(s, s0) < 0;
+      }
+    }
+  return need;
+}
+
+__global__ void __launch_bounds__(256)
+    point_box_kernel(const BoxDesc b, int per_group, signed char *shifts, unsigned char *fallback) {
+  const int rnx = b.rhi[0] - b.rlo[0] + 1, rny = b.rhi[1] - b.rlo[1] + 1;
+  const int64_t rnp = (int64_t)rnx * rny * (b.rhi[2] - b.rlo[2] + 1);
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= rnp)
+    return;
+  const int blk = blockIdx.y; // component (per var) or 0 (per group)
+  const int c0 = per_group ? 0 : blk, c1 = per_group ? b.ncomp : blk + 1;
+  const int ifine[3] = {b.rlo[0] + (int)(idx % rnx), b.rlo[1] + (int)((idx / rnx) % rny),
+                        b.rlo[2] + (int)(idx / ((int64_t)rnx * rny))};
+  Coarse c;
+  c.p = b.crse;
+  c.np = b.cnp;
+  c.nx = b.cnx;
+  c.ny = b.cny;
+  int ic[3], off[3], shift[3], kind[3], lin[3];
+  for (int d = 0; d < 3; ++d) {
+    c.lo[d] = b.clo[d];
+    ic[d] = ifine[d] >> 1; // arithmetic shift = floor, as the reference
+    off[d] = ifine[d] & 1;
+    kind[d] = b.kind[d];
+    const KindInfo ki = kind_info(kind[d]);
+    // linear fallback stencils: impl.hxx:1547-1558 (per var: CONS and ENO
+    // become CONS 1) and 2119-2121 (per group: CONS 1, ENO kept)
+    if (ki.intp == CONS || (!per_group && ki.intp == ENO))
+      lin[d] = K_CC_CONS1;
+    else
+      lin[d] = kind[d];
+  }
+  choose_shift(kind, off, c, c0, c1, ic, shift);
+  double vals[16];
+  for (int comp = c0; comp < c1; ++comp)
+    vals[comp - c0] = eval3d(kind, shift, off, c, comp, ic);
+  bool need = false;
+  if (op_fb_active(b.op, per_group)) {
+    int sr[3][2];
+    for (int d = 0; d < 3; ++d)
+      radius(kind[d], shift[d], off[d], sr[d]);
+    double minval = __longlong_as_double(0x7ff0000000000000LL);
+    double maxval = -minval;
+    for (int comp = c0; comp < c1; ++comp) {
+      // per group the extrema accumulate over the components (impl.hxx:
+      // 2010-2024); per var there is one component
+      for (int dk = sr[2][0]; dk <= sr[2][1]; ++dk)
+        for (int dj = sr[1][0]; dj <= sr[1][1]; ++dj)
+          for (int di = sr[0][0]; di <= sr[0][1]; ++di) {
+            const double x = c(comp, ic[0] + di, ic[1] + dj, ic[2] + dk);
+            minval = fmin(minval, x);
+            maxval = fmax(maxval, x);
+          }
+      need |= vals[comp - c0] < minval || vals[comp - c0] > maxval;
+    }
+    for (int d = 0; d < 3; ++d) {
+      const int intp = kind_info(kind[d]).intp;
+      const bool check = per_group ? intp == CONS : (intp == CONS || intp == ENO);
+      if (!check)
+        continue;
+      for (int comp = c0; comp < c1; ++comp)
+        need |= slope_change(d, sr, c, comp, ic);
+    }
+  }
+  const int64_t fidx = (ifine[0] - b.flo[0]) +
+                       (int64_t)b.fnx * ((ifine[1] - b.flo[1]) + (int64_t)b.fny * (ifine[2] - b.flo[2]));
+  const int zero3[3] = {0, 0, 0};
+  for (int comp = c0; comp < c1; ++comp) {
+    const double res = need ? eval3d(lin, zero3, off, c, comp, ic) : vals[comp - c0];
+    b.fine[comp * b.fnp + fidx] = res;
+  }
+  if (shifts)
+    for (int d = 0; d < 3; ++d)
+      shifts[3 * (blk * rnp + idx) + d] = (signed char)shift[d];
+  if (fallback)
+    fallback[blk * rnp + idx] = need ? 1 : 0;
+}
+
+} // namespace
+
+cudaError_t launch_point_box(const BoxDesc &b, int per_group, signed char *shifts,
+                             unsigned char *fallback, cudaStream_t s) {
+  const int64_t rnp = (int64_t)(b.rhi[0] - b.rlo[0] + 1) * (b.rhi[1] - b.rlo[1] + 1) *
+                      (b.rhi[2] - b.rlo[2] + 1);
+  if (rnp <= 0 || b.ncomp <= 0)
+    return cudaSuccess;
+  const int64_t nblk = (rnp + 255) / 256;
+  if (nblk > INT32_MAX)
+    return cudaErrorInvalidValue;
+  dim3 grid((unsigned)nblk, per_group ? 1 : b.ncomp);
+  point_box_kernel<<<grid, 256, 0, s>>>(b, per_group, shifts, fallback);
+  return cudaGetLastError();
+}
+
+} // namespace cxb

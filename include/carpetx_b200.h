@@ -1,0 +1,181 @@
+/* carpetx_b200 -- B200 (sm_100a) implementation of CarpetX's refinement-factor-2
+ * inter-level transfer operators: the prolongation family of
+ * CarpetX/src/prolongate_3d_rf2* and the restriction CarpetX performs through
+ * AMReX's average_down family.
+ *
+ * C ABI: plain pointers, sizes and status codes; no C++ or torch types.  Every
+ * entry point returns CX_OK (0) or a CX_E* status and never aborts; the C++
+ * amrex::Interpolater shim (carpetx_b200/host/prolongate_3d_rf2_b200.hxx) maps
+ * a non-zero status to CCTK_VERROR, which is the reference's behaviour for
+ * unknown operators (CarpetX/src/driver.cxx:621-625) and failed asserts.
+ *
+ * Data layout, as amrex::FArrayBox: a box is the inclusive index range
+ * [lo, hi] per direction; the ncomp components of a box are stored one after
+ * the other, each Fortran ordered (x fastest), component stride = number of
+ * points of the box.  All values are FP64.  Data pointers are DEVICE pointers
+ * unless stated otherwise; work is enqueued on `stream` and returns without
+ * synchronising, as the reference's GPU path does (impl.hxx:1685-1688).
+ *
+ * Results are bit-identical to the reference operators compiled for the host:
+ * every stencil is evaluated with the reference's association order and
+ * separately rounded products and sums (no FMA contraction). */
+#ifndef CARPETX_B200_H
+#define CARPETX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *cx_stream_t; /* a cudaStream_t; NULL = default */
+
+/* Opaque operator handle (value semantics; equal handles = same operator). */
+typedef int32_t cx_op_t;
+
+enum {
+  CX_OK = 0,
+  CX_EINVAL = 1,       /* bad argument: box, region, ncomp, null pointer */
+  CX_EUNSUPPORTED = 2, /* unknown prolongation type / order / indextype */
+  CX_ECUDA = 3,        /* a CUDA call failed (message: cx_last_error) */
+  CX_ETIMEOUT = 4,     /* a bounded device wait gave up */
+  CX_ENOMEM = 5,       /* scratch or plan allocation failed */
+  CX_ENODEVICE = 6     /* no usable CUDA device */
+};
+
+/* Human-readable name of a status code. */
+const char *cx_status_string(int status);
+/* Text of the most recent failure on this thread ("" if none). */
+const char *cx_last_error(void);
+
+/* ---------------------------------------------------------------------- */
+/* Operator registry                                                       */
+
+/* Replaces get_interpolator(type, order, indextype)
+ * (CarpetX/src/driver.cxx:593-628) and the nine operator tables it indexes
+ * (prolongate_poly/cons/ddf/eno/minmod/hermite/natural/poly_cons3lfb/
+ * poly_eno3lfb_3d_rf2, CarpetX/src/prolongate_3d_rf2.hxx:127-177).
+ * type: "interpolate", "conservative", "ddf", "eno", "minmod", "hermite",
+ * "natural", "poly-cons3lfb", "poly-eno3lfb"; indextype = (cx<<2)|(cy<<1)|cz
+ * with c=1 for cell-centred (driver.cxx:595-596).  CX_EUNSUPPORTED if the
+ * reference has no such operator. */
+int cx_prolong_lookup(const char *type, int order, int indextype,
+                      cx_op_t *out);
+
+/* interp1d<...>::required_ghosts per direction (impl.hxx:398,462,518,585,
+ * 636,783,847). */
+int cx_prolong_required_ghosts(cx_op_t op, int ghosts[3]);
+
+/* prolongate_3d_rf2::CoarseBox (impl.hxx:1236-1254): the fine box coarsened
+ * by 2 (floor) and grown by required_ghosts. */
+int cx_prolong_coarse_box(cx_op_t op, const int fine_lo[3],
+                          const int fine_hi[3], int crse_lo[3],
+                          int crse_hi[3]);
+
+/* ---------------------------------------------------------------------- */
+/* One box (the reference's launch granularity)                            */
+
+/* Replaces prolongate_3d_rf2::interp (impl.hxx:2167-2188): writes the fine
+ * points of reg (inclusive, must lie in the fine box) of ncomp components
+ * from the coarse FAB.  per_group selects interp_per_group (impl.hxx:1691;
+ * CarpetX parameter prolongate_per_group, param.ccl:449-451), which caps
+ * ncomp at 16 and shares the ENO shift and the linear-fallback decision
+ * between components; per_group = 0 is interp_per_var (impl.hxx:1256).  The
+ * coarse FAB must contain every coarse point the stencils read (at most
+ * CoarseBox(reg)); CX_EINVAL otherwise. */
+int cx_prolong_box(cx_op_t op, const double *crse, const int crse_lo[3],
+                   const int crse_hi[3], double *fine, const int fine_lo[3],
+                   const int fine_hi[3], const int reg_lo[3],
+                   const int reg_hi[3], int ncomp, int per_group,
+                   cx_stream_t stream);
+
+/* As cx_prolong_box, and additionally reports, per region point (x fastest)
+ * and per component block (per-var: ncomp blocks, per-group: one), the ENO
+ * shift chosen (3 signed bytes x,y,z; 0 for non-ENO directions) and whether
+ * the linear fallback replaced the value (1 byte).  Either diagnostic
+ * pointer may be NULL.  Diagnostic device arrays; used by the parity tests to
+ * check the stencil choice bit for bit. */
+int cx_prolong_box_diag(cx_op_t op, const double *crse, const int crse_lo[3],
+                        const int crse_hi[3], double *fine,
+                        const int fine_lo[3], const int fine_hi[3],
+                        const int reg_lo[3], const int reg_hi[3], int ncomp,
+                        int per_group, signed char *shifts,
+                        unsigned char *fallback, cx_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
+/* A whole refinement level in one launch                                  */
+
+/* One box of a level transfer: the arguments of one interp() call. */
+typedef struct {
+  cx_op_t op;
+  int ncomp;
+  const double *crse;
+  int crse_lo[3], crse_hi[3];
+  double *fine;
+  int fine_lo[3], fine_hi[3];
+  int reg_lo[3], reg_hi[3];
+} cx_box_t;
+
+typedef struct cx_level_plan *cx_level_plan_t;
+
+/* Builds the device-resident box/tile work list for a set of interp() calls
+ * that would otherwise be one launch per box per component (the loop over
+ * FillPatchInterp's boxes, CarpetX/src/fillpatch.cxx:116-119, 179-180).
+ * Validates every box as cx_prolong_box does, picks the tile shape per box,
+ * sorts tiles by cost and uploads the list (the only allocation).  The
+ * boxes' data pointers are captured by the plan. */
+int cx_level_plan_create(const cx_box_t *boxes, int nboxes, int per_group,
+                         cx_level_plan_t *out);
+/* Enqueues the whole level transfer on stream: one persistent launch per
+ * kernel family present (separable / limited).  Allocates nothing and does
+ * not synchronise, so it can be captured into a CUDA graph. */
+int cx_level_plan_execute(cx_level_plan_t plan, cx_stream_t stream);
+/* Number of tiles and fine points (summed over components) in the plan. */
+int cx_level_plan_stats(cx_level_plan_t plan, int64_t *ntiles,
+                        int64_t *nfine_points, int64_t *algorithmic_bytes);
+/* Frees the plan; the caller ensures no execution is still in flight. */
+int cx_level_plan_destroy(cx_level_plan_t plan);
+
+/* ---------------------------------------------------------------------- */
+/* Restriction                                                             */
+
+/* Replaces the average_down family called by Restrict
+ * (CarpetX/src/schedule.cxx:2793-2815), picked by the number of
+ * cell-centred directions of indextype: nodal (injection), edges, faces,
+ * cells.  For every coarse point c of reg (inclusive, coarse index space):
+ * vertex-centred directions take fine point 2c, cell-centred directions
+ * average the children 2c and 2c+1; children are summed z-outer, x-inner
+ * and the sum is scaled by 1/(number of children). */
+int cx_restrict_box(int indextype, const double *fine, const int fine_lo[3],
+                    const int fine_hi[3], double *crse, const int crse_lo[3],
+                    const int crse_hi[3], const int reg_lo[3],
+                    const int reg_hi[3], int ncomp, cx_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
+/* Adjoints (no reference counterpart: the transposes of the above)        */
+
+/* crse_bar = P^T fine_bar, with P the prolongation of cx_prolong_box
+ * linearised at crse (ENO shift, minmod branch and linear-fallback choice
+ * recomputed from crse).  crse_bar is overwritten over the whole coarse
+ * box (zero where no region point reads).  Gather form, no atomics. */
+int cx_prolong_adjoint_box(cx_op_t op, const double *crse,
+                           const int crse_lo[3], const int crse_hi[3],
+                           const double *fine_bar, const int fine_lo[3],
+                           const int fine_hi[3], const int reg_lo[3],
+                           const int reg_hi[3], int ncomp, int per_group,
+                           double *crse_bar, cx_stream_t stream);
+
+/* fine_bar = R^T crse_bar for cx_restrict_box; fine_bar is overwritten over
+ * the whole fine box. */
+int cx_restrict_adjoint_box(int indextype, const double *crse_bar,
+                            const int crse_lo[3], const int crse_hi[3],
+                            double *fine_bar, const int fine_lo[3],
+                            const int fine_hi[3], const int reg_lo[3],
+                            const int reg_hi[3], int ncomp,
+                            cx_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,201 @@
+"""GPU tests of restriction, the batched level transfer (one persistent launch,
+CUDA-graph capture) and the adjoints, through the C ABI."""
+import numpy as np
+import pytest
+import torch
+
+import carpetx_b200 as cb
+from helpers import assert_bitwise, box_shape, region_mask
+
+pytestmark = pytest.mark.gpu
+
+
+def cuda(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("it", range(8))
+def test_gpu_restrict_matches_oracle(dev, cx, it):
+    rng = np.random.default_rng(100 + it)
+    for _ in range(3):
+        flo = tuple(int(v) for v in rng.integers(-20, 0, 3))
+        fhi = tuple(flo[d] + int(rng.integers(6, 60)) for d in range(3))
+        # coarse region: every coarse point whose children lie in the fine box
+        cc = [(it >> (2 - d)) & 1 for d in range(3)]
+        rlo = tuple(-((-flo[d]) // 2) for d in range(3))
+        rhi = tuple((fhi[d] - cc[d]) // 2 for d in range(3))
+        clo = tuple(rlo[d] - 1 for d in range(3))
+        chi = tuple(rhi[d] + 2 for d in range(3))
+        ncomp = int(rng.integers(1, 4))
+        fine = rng.standard_normal((ncomp,) + box_shape(flo, fhi))
+        want = np.full((ncomp,) + box_shape(clo, chi), np.nan)
+        cx.restrict(it, fine, flo, fhi, want, clo, chi, rlo, rhi, ncomp)
+        got = torch.full(want.shape, np.nan, dtype=torch.float64, device="cuda")
+        cb.restrict_box(it, cuda(fine), flo, fhi, got, clo, chi, rlo, rhi, ncomp)
+        torch.cuda.synchronize()
+        assert_bitwise(got.cpu().numpy(), want, f"indextype {it}")
+
+
+def test_gpu_config2_conservation_round_trip(dev, cx):
+    """Conservative order-2 cell-centred prolongation (conservative order 1,
+    CCC) of a 128^3 box with 3 ghosts, 8 components of random Fourier modes
+    plus noise: bit-identical to the oracle, children average to the coarse
+    value to roundoff, and restriction undoes prolongation."""
+    from carpetx_b200.workloads import fourier_fab
+    clo, chi = (-3, -3, -3), (130, 130, 130)
+    flo, fhi = (0, 0, 0), (255, 255, 255)
+    crse = fourier_fab(np.random.default_rng(2), 8, clo, chi)
+    g_crse = cuda(crse)
+    g_fine = torch.empty((8,) + box_shape(flo, fhi), dtype=torch.float64, device="cuda")
+    op = cb.Op("conservative", 1, 7)
+    for pg in (0, 1):
+        cb.prolong_box(op, g_crse, clo, chi, g_fine, flo, fhi, flo, fhi, 8, per_group=pg)
+        torch.cuda.synchronize()
+        if pg == 0:
+            want = np.empty((8,) + box_shape(flo, fhi))
+            cx.prolong("conservative", 1, 7, 0, crse, clo, chi, want, flo, fhi, flo, fhi, 8)
+            assert_bitwise(g_fine.cpu().numpy(), want, "config 2 prolongation")
+            del want
+        back = torch.empty_like(g_crse)
+        cb.restrict_box(7, g_fine, flo, fhi, back, clo, chi, (0, 0, 0), (127, 127, 127), 8)
+        torch.cuda.synchronize()
+        inner = (slice(None),) + (slice(3, 131),) * 3
+        err = (back[inner] - g_crse[inner]).abs().max().item()
+        assert err <= 4 * np.finfo(float).eps * g_crse[inner].abs().max().item()
+
+
+def mixed_level(rng, nboxes, ncomp, cx=None, smin=4, smax=20):
+    """Boxes with log-uniform sizes, 3 ghosts, centrings VVV/CCC/VVC/VCC:
+    poly order 5 for VVV, hermite order 3 otherwise."""
+    boxes = []
+    for b in range(nboxes):
+        n = np.round(np.exp(rng.uniform(np.log(smin), np.log(smax), 3))).astype(int)
+        it = int(rng.choice([0, 7, 1, 3]))
+        typ, order = ("interpolate", 5) if it == 0 else ("hermite", 3)
+        cc = [(it >> (2 - d)) & 1 for d in range(3)]
+        # coarse cells 0..n-1 (+1 vertex in VC directions), fine = 2n (+1)
+        flo = (0, 0, 0)
+        fhi = tuple(int(2 * n[d] - 1 + (1 - cc[d])) for d in range(3))
+        clo = (-3, -3, -3)
+        chi = tuple(int(n[d] - 1 + (1 - cc[d]) + 3) for d in range(3))
+        crse = rng.standard_normal((ncomp,) + box_shape(clo, chi))
+        boxes.append(dict(typ=typ, order=order, it=it, op=cb.Op(typ, order, it), ncomp=ncomp,
+                          crse_np=crse, crse_lo=clo, crse_hi=chi, fine_lo=flo, fine_hi=fhi,
+                          reg_lo=flo, reg_hi=fhi))
+    return boxes
+
+
+def test_gpu_level_plan_matches_per_box(dev, cx):
+    rng = np.random.default_rng(9)
+    boxes = mixed_level(rng, 24, 3)
+    for b in boxes:
+        b["crse"] = cuda(b["crse_np"])
+        b["fine"] = torch.full((3,) + box_shape(b["fine_lo"], b["fine_hi"]), np.nan,
+                               dtype=torch.float64, device="cuda")
+    plan = cb.LevelPlan(boxes)
+    st = plan.stats()
+    assert st["fine_points"] == sum(3 * np.prod(box_shape(b["fine_lo"], b["fine_hi"]))
+                                    for b in boxes)
+    plan.execute()
+    torch.cuda.synchronize()
+    for b in boxes:
+        want = np.full((3,) + box_shape(b["fine_lo"], b["fine_hi"]), np.nan)
+        cx.prolong(b["typ"], b["order"], b["it"], 0, b["crse_np"], b["crse_lo"], b["crse_hi"],
+                   want, b["fine_lo"], b["fine_hi"], b["reg_lo"], b["reg_hi"], 3)
+        assert_bitwise(b["fine"].cpu().numpy(), want, f"level box {b['typ']} it{b['it']}")
+    # replay under a captured CUDA graph
+    for b in boxes:
+        b["fine"].fill_(np.nan)
+    s = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        plan.execute(stream=s)
+    g.replay()
+    g.replay()
+    torch.cuda.synchronize()
+    for b in boxes:
+        want = np.full((3,) + box_shape(b["fine_lo"], b["fine_hi"]), np.nan)
+        cx.prolong(b["typ"], b["order"], b["it"], 0, b["crse_np"], b["crse_lo"], b["crse_hi"],
+                   want, b["fine_lo"], b["fine_hi"], b["reg_lo"], b["reg_hi"], 3)
+        assert_bitwise(b["fine"].cpu().numpy(), want, "graph replay")
+    plan.close()
+
+
+def test_gpu_level_plan_limited_and_empty(dev, cx):
+    """A level mixing separable and limited (ENO, fallback) boxes and an empty
+    region."""
+    rng = np.random.default_rng(4)
+    specs = [("eno", 3, 7), ("interpolate", 3, 0), ("poly-cons3lfb", 3, 7), ("minmod", 1, 7)]
+    boxes = []
+    for typ, order, it in specs:
+        flo, fhi = (-4, -4, -4), (21, 17, 13)
+        clo, chi = cx.coarse_box(typ, order, it, flo, fhi)
+        crse = rng.standard_normal((2,) + box_shape(clo, chi))
+        boxes.append(dict(typ=typ, order=order, it=it, op=cb.Op(typ, order, it), ncomp=2,
+                          crse_np=crse, crse=cuda(crse), crse_lo=clo, crse_hi=chi,
+                          fine=torch.full((2,) + box_shape(flo, fhi), np.nan, dtype=torch.float64,
+                                          device="cuda"),
+                          fine_lo=flo, fine_hi=fhi, reg_lo=flo, reg_hi=fhi))
+    e = dict(boxes[1], reg_lo=(0, 0, 0), reg_hi=(-1, 5, 5))
+    plan = cb.LevelPlan(boxes + [e])
+    plan.execute()
+    torch.cuda.synchronize()
+    for b in boxes:
+        want = np.full((2,) + box_shape(b["fine_lo"], b["fine_hi"]), np.nan)
+        cx.prolong(b["typ"], b["order"], b["it"], 0, b["crse_np"], b["crse_lo"], b["crse_hi"],
+                   want, b["fine_lo"], b["fine_hi"], b["reg_lo"], b["reg_hi"], 2)
+        assert_bitwise(b["fine"].cpu().numpy(), want, f"{b['typ']}")
+    plan.close()
+
+
+@pytest.mark.parametrize("typ,order,it", [("interpolate", 5, 0), ("conservative", 1, 7),
+                                          ("natural", 3, 3), ("ddf", 7, 6), ("hermite", 5, 1),
+                                          ("interpolate", 7, 7), ("conservative", 0, 2)])
+def test_gpu_prolong_adjoint(dev, cx, typ, order, it):
+    """Dot-product test <P u, v> = <u, P^T v> to 1e-13 relative, and P^T
+    against the oracle's transpose."""
+    rng = np.random.default_rng(order * 8 + it)
+    flo, fhi = (-5, -3, 2), (30, 27, 21)
+    rlo, rhi = (-4, -3, 3), (29, 27, 20)
+    clo, chi = cx.coarse_box(typ, order, it, rlo, rhi)
+    op = cb.Op(typ, order, it)
+    u = rng.standard_normal((2,) + box_shape(clo, chi))
+    v = rng.standard_normal((2,) + box_shape(flo, fhi)) * region_mask(flo, fhi, rlo, rhi)
+    gu, gv = cuda(u), cuda(v)
+    Pu = torch.zeros_like(gv)
+    cb.prolong_box(op, gu, clo, chi, Pu, flo, fhi, rlo, rhi, 2)
+    PTv = torch.full_like(gu, np.nan)
+    cb.prolong_adjoint_box(op, gu, clo, chi, gv, flo, fhi, rlo, rhi, 2, PTv)
+    torch.cuda.synchronize()
+    lhs = torch.sum(Pu * gv).item()
+    rhs = torch.sum(gu * PTv).item()
+    scale = torch.sum(torch.abs(Pu * gv)).item()
+    assert abs(lhs - rhs) <= 1e-13 * scale, (lhs, rhs)
+    want = np.zeros_like(u)
+    cx.prolong_adjoint(typ, order, it, 0, u, clo, chi, v, flo, fhi, rlo, rhi, 2, want)
+    np.testing.assert_allclose(PTv.cpu().numpy(), want, rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("it", [0, 7, 3])
+def test_gpu_restrict_adjoint(dev, cx, it):
+    rng = np.random.default_rng(it)
+    flo, fhi = (0, 0, 0), (23, 21, 19)
+    rlo, rhi = (0, 0, 0), (11, 10, 9)
+    clo, chi = (-2, -2, -2), (13, 12, 11)
+    f = rng.standard_normal((2,) + box_shape(flo, fhi))
+    g = rng.standard_normal((2,) + box_shape(clo, chi))
+    Rf = torch.zeros((2,) + box_shape(clo, chi), dtype=torch.float64, device="cuda")
+    cb.restrict_box(it, cuda(f), flo, fhi, Rf, clo, chi, rlo, rhi, 2)
+    RTg = torch.full((2,) + box_shape(flo, fhi), np.nan, dtype=torch.float64, device="cuda")
+    cb.restrict_adjoint_box(it, cuda(g), clo, chi, RTg, flo, fhi, rlo, rhi, 2)
+    torch.cuda.synchronize()
+    mask = np.zeros(g.shape, bool)
+    mask[:, rlo[2] - clo[2]:rhi[2] - clo[2] + 1, rlo[1] - clo[1]:rhi[1] - clo[1] + 1,
+         rlo[0] - clo[0]:rhi[0] - clo[0] + 1] = True
+    lhs = np.sum(Rf.cpu().numpy() * g * mask)
+    rhs = np.sum(f * RTg.cpu().numpy())
+    assert abs(lhs - rhs) <= 1e-13 * np.sum(np.abs(f)) * np.max(np.abs(g))
+    want = np.zeros_like(f)
+    cx.restrict_adjoint(it, g, clo, chi, want, flo, fhi, rlo, rhi, 2)
+    np.testing.assert_array_equal(RTg.cpu().numpy(), want)
