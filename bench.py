@@ -1,0 +1,428 @@
+"""Benchmark of the batched level prolongation (FP64 fine points per second).
+
+Workload (default, "level512"): one refinement level of 512 boxes, coarse cells
+per direction round(exp(U[ln 8, ln 64])) (seeded), 3 ghost zones, 24 FP64
+variables per var (per-component transfers), centrings uniform over VVV, CCC,
+VVC, VCC; VVV boxes use "interpolate" order 5, the staggered ones "hermite"
+order 3.  Synthetic data (seeded normal values; the operators are linear, the
+values do not change the work).
+
+One step = prolongation of every box and component of the level.  Reported:
+  value      fine points/s of the batched transfer (one persistent launch,
+             replayed from a CUDA graph), inputs resident in HBM
+  per_box    the same work launched once per box per component (the
+             reference's launch granularity), our kernel
+  e2e        through the C ABI with host buffers: pinned host -> device copy
+             of the coarse data, the level transfer, device -> host copy of
+             the fine data, every step
+  roofline   algorithmic bytes 8 (|CoarseBox(region)| + |region|) per box and
+             component over the kernel time, against the measured HBM copy
+             bandwidth
+  cpu_baseline  the reference operators compiled for the host
+             (oracle/_ref, all host threads, OpenMP over boxes) on one
+             component of every box
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FP64 fine points/s, batched persistent level prolongation"
+UNIT = "fine points/s"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="level512", choices=["level512", "cons128"])
+    p.add_argument("--seed", type=int, default=2026)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--per-box-steps", type=int, default=2)
+    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--boxes", type=int, default=512, help="level512: number of boxes")
+    p.add_argument("--ncomp", type=int, default=24, help="level512: variables per box")
+    return p.parse_args()
+
+
+def box_shape(lo, hi):
+    return tuple(int(hi[d]) - int(lo[d]) + 1 for d in (2, 1, 0))
+
+
+def npts(lo, hi):
+    return int(np.prod(box_shape(lo, hi)))
+
+
+def workload(name, seed, nboxes=512, ncomp=24):
+    """List of boxes (type, order, indextype, crse_lo, crse_hi, fine_lo, fine_hi,
+    ncomp) and a description."""
+    from carpetx_b200.workloads import mixed_level_boxes
+    if name == "level512":
+        out = []
+        for it, clo, chi, flo, fhi in mixed_level_boxes(seed, nboxes=nboxes):
+            typ, order = ("interpolate", 5) if it == 0 else ("hermite", 3)
+            out.append((typ, order, it, clo, chi, flo, fhi, ncomp))
+        return out, {"workload": f"level512: {nboxes} boxes, coarse 8-64 cells/dim log-uniform, "
+                                 f"3 ghosts, {ncomp} vars per var, VVV interpolate o5 / "
+                                 "VVC,VCC,CCC hermite o3",
+                     "boxes": nboxes, "ncomp": ncomp}
+    # one 128^3-cell box, 3 ghosts, 8 vars, conservative order 1 (CC CONS 2)
+    return ([("conservative", 1, 7, (-3, -3, -3), (130, 130, 130), (0, 0, 0), (255, 255, 255), 8)],
+            {"workload": "cons128: conservative o1 CCC, 128^3 -> 256^3 cells, 3 ghosts, 8 vars",
+             "boxes": 1, "ncomp": 8})
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+# --------------------------------------------------------------------------
+# CPU baseline: the reference operators compiled for the host
+
+def cpu_lib():
+    """(ctypes lib, kind): oracle/_ref (the reference itself) if built, else
+    the oracle port."""
+    from oracle.oracle import RefOracle, CxOracle
+    if RefOracle.available(fast=True):
+        L = RefOracle(fast=True).lib
+        L.ref_prolong_many.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
+                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                       ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_void_p),
+                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int)]
+        return L, "reference"
+    return CxOracle(), "port"
+
+
+def cpu_sample(boxes, seed, ncomp_sample=1):
+    """Host FABs for one component of every box (the bounded CPU sample)."""
+    rng = np.random.default_rng(seed)
+    crse, fine = [], []
+    for (typ, order, it, clo, chi, flo, fhi, n) in boxes:
+        crse.append(rng.standard_normal((ncomp_sample,) + box_shape(clo, chi)))
+        fine.append(np.empty((ncomp_sample,) + box_shape(flo, fhi)))
+    return crse, fine
+
+
+def cpu_run(lib, kind, boxes, crse, fine, ncomp_sample=1):
+    """One pass of the reference CPU path over the sample; returns seconds."""
+    n = len(boxes)
+    t0 = time.perf_counter()
+    if kind == "reference":
+        I = ctypes.c_int
+        types = (ctypes.c_char_p * n)(*[b[0].encode() for b in boxes])
+        orders = (I * n)(*[b[1] for b in boxes])
+        its = (I * n)(*[b[2] for b in boxes])
+        cp = (ctypes.c_void_p * n)(*[c.ctypes.data for c in crse])
+        fp = (ctypes.c_void_p * n)(*[f.ctypes.data for f in fine])
+        flat = lambda k: (I * (3 * n))(*[v for b in boxes for v in b[k]])  # noqa: E731
+        nc = (I * n)(*([ncomp_sample] * n))
+        t0 = time.perf_counter()
+        rc = lib.ref_prolong_many(n, types, orders, its, 0, cp, flat(3), flat(4), fp, flat(5),
+                                  flat(6), flat(5), flat(6), nc)
+        assert rc == 0
+    else:
+        for b, c, f in zip(boxes, crse, fine):
+            lib.prolong(b[0], b[1], b[2], 0, c, b[3], b[4], f, b[5], b[6], b[5], b[6],
+                        ncomp_sample)
+    return time.perf_counter() - t0
+
+
+def cpu_threads():
+    return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+
+
+def run_reference(args, rank):
+    """--impl reference: the reference's own CPU implementation of the path on
+    the host cores, same workload, one component of every box per step."""
+    if rank != 0:
+        return
+    boxes, cfg = workload(args.workload, args.seed, args.boxes, args.ncomp)
+    lib, kind = cpu_lib()
+    crse, fine = cpu_sample(boxes, args.seed)
+    pts = sum(npts(b[5], b[6]) for b in boxes)
+    for _ in range(args.warmup):
+        cpu_run(lib, kind, boxes, crse, fine)
+    ts = [cpu_run(lib, kind, boxes, crse, fine) for _ in range(args.steps)]
+    t = float(np.sum(ts))
+    value = pts * args.steps / t
+    cores = cpu_threads() if kind == "reference" else cpu_threads()
+    sample = f"component 0 of all {len(boxes)} boxes ({pts} fine points) per step"
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------
+# GPU arm
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+    import carpetx_b200 as cb
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    # weak scaling: every rank transfers its own level (seed + rank); the
+    # boxes are independent, so there is no data-path collective
+    boxes, cfg = workload(args.workload, args.seed + rank, args.boxes, args.ncomp)
+    coff, foff, ctot, ftot = [], [], 0, 0
+    for b in boxes:
+        coff.append(ctot)
+        foff.append(ftot)
+        ctot += b[7] * npts(b[3], b[4])
+        ftot += b[7] * npts(b[5], b[6])
+    crse = torch.empty(ctot, dtype=torch.float64, device=dev)
+    fine = torch.empty(ftot, dtype=torch.float64, device=dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(args.seed + rank)
+    crse.normal_(generator=gen)
+    lb = []
+    for b, co, fo in zip(boxes, coff, foff):
+        typ, order, it, clo, chi, flo, fhi, n = b
+        lb.append(dict(op=cb.Op(typ, order, it), ncomp=n,
+                       crse=crse[co:co + n * npts(clo, chi)].view((n,) + box_shape(clo, chi)),
+                       crse_lo=clo, crse_hi=chi,
+                       fine=fine[fo:fo + n * npts(flo, fhi)].view((n,) + box_shape(flo, fhi)),
+                       fine_lo=flo, fine_hi=fhi, reg_lo=flo, reg_hi=fhi))
+    plan = cb.LevelPlan(lb)
+    st = plan.stats()
+    nfine = st["fine_points"]
+    alg_bytes = st["bytes"]
+    stream = torch.cuda.Stream(device=dev)
+
+    # capture the level transfer as a CUDA graph
+    with torch.cuda.stream(stream):
+        plan.execute(stream)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        plan.execute(stream)
+    for _ in range(args.warmup):
+        graph.replay()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return t.item()
+
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    time.sleep(0.3)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with torch.cuda.stream(stream):
+        ev[0].record(stream)
+        for k in range(args.steps):
+            graph.replay()
+            ev[k + 1].record(stream)
+    barrier()
+    clk = clocks.stop()
+    per_step = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    ms_total = max_over_ranks(ev[0].elapsed_time(ev[-1]))
+    ms_step = ms_total / args.steps
+    value = world * nfine * args.steps / (ms_total / 1e3)
+
+    # the same work launched once per box per component (our kernel)
+    L = cb.lib()
+    I3 = ctypes.c_int * 3
+    calls = []
+    for b in lb:
+        n = b["ncomp"]
+        cs = npts(b["crse_lo"], b["crse_hi"])
+        fs = npts(b["fine_lo"], b["fine_hi"])
+        for c in range(n):
+            calls.append((b["op"].handle, ctypes.c_void_p(b["crse"].data_ptr() + 8 * c * cs),
+                          I3(*b["crse_lo"]), I3(*b["crse_hi"]),
+                          ctypes.c_void_p(b["fine"].data_ptr() + 8 * c * fs),
+                          I3(*b["fine_lo"]), I3(*b["fine_hi"]), I3(*b["reg_lo"]),
+                          I3(*b["reg_hi"])))
+    sp = ctypes.c_void_p(stream.cuda_stream)
+
+    def per_box_step():
+        for c in calls:
+            rc = L.cx_prolong_box(*c, 1, 0, sp)
+            if rc:
+                raise RuntimeError(L.cx_last_error().decode())
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms_pb, per_box_value = None, None
+    if args.per_box_steps > 0:
+        per_box_step()
+        torch.cuda.synchronize()
+        barrier()
+        e0.record(stream)
+        for _ in range(args.per_box_steps):
+            per_box_step()
+        e1.record(stream)
+        barrier()
+        ms_pb = max_over_ranks(e0.elapsed_time(e1)) / args.per_box_steps
+        per_box_value = world * nfine / (ms_pb / 1e3)
+
+    # end to end through the C ABI with host buffers
+    ms_e2e, e2e_value = None, None
+    if args.e2e_steps > 0:
+        h_crse = torch.empty(ctot, dtype=torch.float64, pin_memory=True)
+        h_fine = torch.empty(ftot, dtype=torch.float64, pin_memory=True)
+        h_crse.copy_(crse.cpu())
+        barrier()
+        e0.record(stream)
+        with torch.cuda.stream(stream):
+            for _ in range(args.e2e_steps):
+                crse.copy_(h_crse, non_blocking=True)
+                plan.execute(stream)
+                h_fine.copy_(fine, non_blocking=True)
+        e1.record(stream)
+        barrier()
+        ms_e2e = max_over_ranks(e0.elapsed_time(e1)) / args.e2e_steps
+        e2e_value = world * nfine / (ms_e2e / 1e3)
+
+    peak, peak_src = measured_peaks()
+    achieved = alg_bytes / (ms_step / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(cfg, fine_points_per_gpu=nfine, algorithmic_bytes_per_gpu=alg_bytes,
+                       l2_flush=f"inputs+outputs {(8 * (ctot + ftot)) / 1e9:.1f} GB per GPU "
+                                f">> L2 ({L2_BYTES / 2**20:.0f} MiB); no explicit flush",
+                       parallelism=f"weak: one independent level per GPU x{world}",
+                       launch="one persistent kernel per step, CUDA graph replay"),
+        "gpu_launches": args.steps,
+        "per_box": {"value": per_box_value, "unit": UNIT, "ms_per_step": ms_pb,
+                    "launches_per_step": len(calls),
+                    "batched_speedup": value / per_box_value if per_box_value else None},
+        "e2e": {"value": e2e_value, "unit": UNIT, "ms_per_step": ms_e2e,
+                "h2d_bytes_per_step": 8 * ctot, "d2h_bytes_per_step": 8 * ftot},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": peak_src,
+                     "frac_of_8TBs_spec": achieved / 8000.0,
+                     "step_ms_min": min(per_step), "step_ms_max": max(per_step)},
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        lib, kind = cpu_lib()
+        cboxes = boxes
+        c_crse, c_fine = cpu_sample(cboxes, args.seed)
+        cpu_run(lib, kind, cboxes, c_crse, c_fine)  # warm-up
+        t = cpu_run(lib, kind, cboxes, c_crse, c_fine)
+        pts = sum(npts(b[5], b[6]) for b in cboxes)
+        line["cpu_baseline"] = {"value": pts / t, "unit": UNIT, "cores": cpu_threads(),
+                                "kind": kind,
+                                "sample": f"component 0 of all {len(cboxes)} boxes "
+                                          f"({pts} fine points), one pass after one warm-up"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.close()
+    del graph
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

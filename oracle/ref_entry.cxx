@@ -74,6 +74,36 @@ int ref_coarse_box(const char *type, int order, int indextype,
   return 0;
 }
 
+/* Runs the reference interp() on n boxes, one OpenMP task per box (the
+ * reference parallelises over boxes/tiles with OpenMP around interp, as
+ * AMReX's MFIter does).  Arrays are indexed per box; boxes are 3 ints each.
+ * Used for the CPU-baseline timing. */
+int ref_prolong_many(int n, const char *const *types, const int *orders,
+                     const int *indextypes, int per_group,
+                     const double *const *crse, const int *crse_lo,
+                     const int *crse_hi, double *const *fine,
+                     const int *fine_lo, const int *fine_hi, const int *reg_lo,
+                     const int *reg_hi, const int *ncomp) {
+  for (int b = 0; b < n; ++b)
+    if (!lookup(types[b], orders[b], indextypes[b]))
+      return -1;
+  cx_ref_prolongate_per_group = per_group;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int b = 0; b < n; ++b) {
+    amrex::Interpolater *op = lookup(types[b], orders[b], indextypes[b]);
+    amrex::FArrayBox cfab(mkbox(crse_lo + 3 * b, crse_hi + 3 * b),
+                          const_cast<double *>(crse[b]), ncomp[b]);
+    amrex::FArrayBox ffab(mkbox(fine_lo + 3 * b, fine_hi + 3 * b), fine[b],
+                          ncomp[b]);
+    const amrex::Vector<amrex::BCRec> bcr;
+    op->interp(cfab, 0, ffab, 0, ncomp[b],
+               mkbox(reg_lo + 3 * b, reg_hi + 3 * b), amrex::IntVect(2, 2, 2),
+               amrex::Geometry(), amrex::Geometry(), bcr, 0, 0,
+               amrex::RunOn::Cpu);
+  }
+  return 0;
+}
+
 /* Runs the reference interp() (impl.hxx:2167-2188) on host FABs.  crse/fine
  * hold ncomp components, each of box.numPts() doubles, x fastest. */
 int ref_prolong(const char *type, int order, int indextype, int per_group,
