@@ -123,7 +123,6 @@ int make_box(cx_op_t op, const double *crse, const int clo[3], const int chi[3],
   b->fine = fine;
   b->op = op;
   b->ncomp = ncomp;
-  const int T[3] = {kSepTX, kSepTY, kSepTZ};
   for (int d = 0; d < 3; ++d) {
     const int k = op_kind(op, d);
     b->kind[d] = k;
@@ -150,8 +149,6 @@ int make_box(cx_op_t op, const double *crse, const int clo[3], const int chi[3],
                   clo[d], chi[d], nlo, nhi, d);
     b->nlo[d] = nlo;
     b->nhi[d] = nhi;
-    b->tbase[d] = rlo[d] & ~1;
-    b->ntile[d] = (rhi[d] - b->tbase[d] + T[d]) / T[d];
   }
   b->cnx = chi[0] - clo[0] + 1;
   b->cny = chi[1] - clo[1] + 1;
@@ -159,6 +156,7 @@ int make_box(cx_op_t op, const double *crse, const int clo[3], const int chi[3],
   b->fnx = fhi[0] - flo[0] + 1;
   b->fny = fhi[1] - flo[1] + 1;
   b->fnp = (int64_t)b->fnx * b->fny * (fhi[2] - flo[2] + 1);
+  stream_tiling(*b);
   (void)per_group;
   return CX_OK;
 }
@@ -184,11 +182,10 @@ struct cx_level_plan {
   std::vector<int> point_boxes; // boxes handled by the pointwise kernel
   BoxDesc *d_boxes = nullptr;
   TileRef *d_tiles = nullptr;
-  int *d_counter = nullptr;
   int nsep_tiles = 0;
-  int s0max = 0, s1max = 0;
-  size_t smem = 0;
-  int grid = 0;
+  // items of z-window group g: [group_off[g], group_off[g + 1]) of d_tiles
+  int group_off[kStrGroups + 1] = {};
+  int group_grid[kStrGroups] = {};
   int64_t nfine = 0, bytes = 0;
 };
 
@@ -262,7 +259,7 @@ int cx_prolong_box_diag(cx_op_t op, const double *crse, const int crse_lo[3], co
     return e;
   cudaStream_t s = (cudaStream_t)stream;
   if (op_separable(op, per_group) && !shifts && !fallback)
-    return cuda_status(launch_sep_box(b, s), "prolongation launch");
+    return cuda_status(launch_stream_box(b, s), "prolongation launch");
   if (op_separable(op, per_group)) {
     // diagnostics requested for an operator without shifts or fallback:
     // values from the separable kernel, diagnostics all zero
@@ -273,7 +270,7 @@ int cx_prolong_box_diag(cx_op_t op, const double *crse, const int crse_lo[3], co
     if (fallback)
       if (int e = cuda_status(cudaMemsetAsync(fallback, 0, nreg, s), "memset"))
         return e;
-    return cuda_status(launch_sep_box(b, s), "prolongation launch");
+    return cuda_status(launch_stream_box(b, s), "prolongation launch");
   }
   return cuda_status(launch_point_box(b, per_group, shifts, fallback, s), "prolongation launch");
 }
@@ -305,9 +302,13 @@ int cx_level_plan_create(const cx_box_t *boxes, int nboxes, int per_group, cx_le
     }
     if (empty)
       continue;
-    int g[3], cl[3], ch[3];
+    if (b.ntile[0] > INT16_MAX || b.ntile[1] > INT16_MAX || b.ntile[2] > INT16_MAX ||
+        x.ncomp > INT16_MAX) {
+      delete p;
+      return fail(CX_EINVAL, "box %d: too many tiles or components for a level plan", i);
+    }
+    int cl[3], ch[3];
     cx_prolong_coarse_box(x.op, x.reg_lo, x.reg_hi, cl, ch);
-    (void)g;
     p->nfine += box_points(x.reg_lo, x.reg_hi) * x.ncomp;
     p->bytes += 8 * (box_points(cl, ch) + box_points(x.reg_lo, x.reg_hi)) * x.ncomp;
     const int id = (int)p->boxes.size();
@@ -317,31 +318,38 @@ int cx_level_plan_create(const cx_box_t *boxes, int nboxes, int per_group, cx_le
     else
       p->point_boxes.push_back(id);
   }
-  // tiles of the separable boxes, largest boxes first (longest-processing-
-  // time order for the dynamic scheduler), x fastest within a box
-  std::sort(sep_ids.begin(), sep_ids.end(), [&](int a, int b) {
-    const BoxDesc &A = p->boxes[a], &B = p->boxes[b];
-    const int64_t na = (int64_t)A.ntile[0] * A.ntile[1] * A.ntile[2];
-    const int64_t nb = (int64_t)B.ntile[0] * B.ntile[1] * B.ntile[2];
-    return na != nb ? na > nb : a < b;
-  });
-  std::vector<TileRef> tiles;
+  // work items of the separable boxes: (box, x tile, y tile, z chunk,
+  // component), sorted by streamed planes, largest first; the kernel deals
+  // them round-robin to its persistent CTAs
+  std::vector<std::pair<int, TileRef>> keyed;
   for (int id : sep_ids) {
     const BoxDesc &b = p->boxes[id];
-    const SepSmem m = sep_smem_for(b.kind);
-    p->s0max = std::max(p->s0max, m.s0);
-    p->s1max = std::max(p->s1max, m.s1);
-    p->smem = std::max(p->smem, (size_t)0);
+    const int L = sep_rhi(b.kind[2]) - sep_rlo(b.kind[2]);
     for (int c = 0; c < b.ncomp; ++c)
-      for (int tz = 0; tz < b.ntile[2]; ++tz)
+      for (int tz = 0; tz < b.ntile[2]; ++tz) {
+        const int z0 = b.tbase[2] + tz * b.zchunk;
+        const int z1 = std::min(z0 + b.zchunk - 1, b.rhi[2]);
+        const int planes = (z1 >> 1) - (z0 >> 1) + 1 + L;
         for (int ty = 0; ty < b.ntile[1]; ++ty)
           for (int tx = 0; tx < b.ntile[0]; ++tx)
-            tiles.push_back(TileRef{id, (int16_t)tx, (int16_t)ty, (int16_t)tz, (int16_t)c});
+            keyed.push_back({planes, TileRef{id, (int16_t)tx, (int16_t)ty, (int16_t)tz, (int16_t)c}});
+      }
   }
-  int s2max = 0;
-  for (int id : sep_ids)
-    s2max = std::max(s2max, sep_smem_for(p->boxes[id].kind).s2);
-  p->smem = sizeof(double) * (size_t)(2 * p->s0max + p->s1max + s2max);
+  // by z-window group (one kernel each), then by cost, largest first
+  auto group_of = [&](const TileRef &t) { return stream_zgroup(p->boxes[t.box].kind[2]); };
+  std::stable_sort(keyed.begin(), keyed.end(),
+                   [&](const std::pair<int, TileRef> &a, const std::pair<int, TileRef> &b) {
+                     const int ga = group_of(a.second), gb = group_of(b.second);
+                     return ga != gb ? ga < gb : a.first > b.first;
+                   });
+  for (auto &k : keyed)
+    p->group_off[group_of(k.second) + 1]++;
+  for (int g = 0; g < kStrGroups; ++g)
+    p->group_off[g + 1] += p->group_off[g];
+  std::vector<TileRef> tiles;
+  tiles.reserve(keyed.size());
+  for (auto &k : keyed)
+    tiles.push_back(k.second);
   if (tiles.size() > (size_t)INT32_MAX) {
     delete p;
     return fail(CX_EINVAL, "too many tiles");
@@ -352,8 +360,6 @@ int cx_level_plan_create(const cx_box_t *boxes, int nboxes, int per_group, cx_le
     e = cudaMalloc(&p->d_boxes, sizeof(BoxDesc) * p->boxes.size());
   if (e == cudaSuccess && !tiles.empty())
     e = cudaMalloc(&p->d_tiles, sizeof(TileRef) * tiles.size());
-  if (e == cudaSuccess)
-    e = cudaMalloc(&p->d_counter, sizeof(int));
   if (e == cudaSuccess && !p->boxes.empty())
     e = cudaMemcpy(p->d_boxes, p->boxes.data(), sizeof(BoxDesc) * p->boxes.size(),
                    cudaMemcpyHostToDevice);
@@ -365,7 +371,8 @@ int cx_level_plan_create(const cx_box_t *boxes, int nboxes, int per_group, cx_le
     return fail(e == cudaErrorMemoryAllocation ? CX_ENOMEM : CX_ECUDA, "level plan: %s",
                 cudaGetErrorString(e));
   }
-  p->grid = p->nsep_tiles ? sep_level_grid(p->smem) : 0;
+  for (int g = 0; g < kStrGroups; ++g)
+    p->group_grid[g] = p->group_off[g + 1] > p->group_off[g] ? stream_level_grid(g) : 0;
   *out = p;
   return CX_OK;
 }
@@ -374,11 +381,14 @@ int cx_level_plan_execute(cx_level_plan_t p, cx_stream_t stream) {
   if (!p)
     return fail(CX_EINVAL, "null plan");
   cudaStream_t s = (cudaStream_t)stream;
-  if (p->nsep_tiles)
-    if (int e = cuda_status(launch_sep_level(p->d_boxes, p->d_tiles, p->nsep_tiles, p->d_counter,
-                                             p->s0max, p->s1max, p->smem, p->grid, s),
-                            "level launch"))
-      return e;
+  for (int g = 0; g < kStrGroups; ++g) {
+    const int n = p->group_off[g + 1] - p->group_off[g];
+    if (n > 0)
+      if (int e = cuda_status(launch_stream_level(g, p->d_boxes, p->d_tiles + p->group_off[g], n,
+                                                  p->group_grid[g], s),
+                              "level launch"))
+        return e;
+  }
   for (int id : p->point_boxes)
     if (int e = cuda_status(launch_point_box(p->boxes[id], p->per_group, nullptr, nullptr, s),
                             "level launch (limited operators)"))
@@ -403,7 +413,6 @@ int cx_level_plan_destroy(cx_level_plan_t p) {
     return CX_OK;
   cudaFree(p->d_boxes);
   cudaFree(p->d_tiles);
-  cudaFree(p->d_counter);
   delete p;
   return CX_OK;
 }

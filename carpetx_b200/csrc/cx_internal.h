@@ -7,10 +7,10 @@
 
 namespace cxb {
 
-// Fine tile of the separable kernel (fine points per direction).  The tile
-// origin is even in every direction, so fine offset = local index & 1.
-constexpr int kSepTX = 32, kSepTY = 8, kSepTZ = 8;
-constexpr int kSepThreads = 256;
+// Column of the streaming kernel: kStrX x kStrY fine points in x and y, fine
+// z in chunks of BoxDesc::zchunk; kStrFY fine y per thread.
+constexpr int kStrX = 32, kStrY = 16, kStrFY = 2;
+constexpr int kStrThreads = kStrX * kStrY / kStrFY;
 
 // One box of a transfer as the kernels see it.  Coordinates are AMReX index
 // space; strides in elements.
@@ -24,11 +24,13 @@ struct BoxDesc {
   int fnx, fny;       // fine FAB extents in x, y
   int rlo[3], rhi[3]; // fine region (inclusive)
   int nlo[3], nhi[3]; // coarse points the operator reads (inclusive)
-  int tbase[3];       // tile origin base: rlo rounded down to even
-  int ntile[3];       // tiles per direction
+  int tbase[3];       // tile origin base: rlo rounded down to even (the
+                      // tile origin is even, so fine offset = local & 1)
+  int ntile[3];       // tiles per direction (streaming kernel: x, y, z chunks)
   int kind[3];        // 1-D stencil kind per direction
   int op;             // operator handle
   int ncomp;
+  int zchunk;         // streaming kernel: fine z per item (even)
 };
 
 // One unit of work of the level kernel: a tile of a box, one component.
@@ -38,22 +40,19 @@ struct TileRef {
   int16_t comp;
 };
 
-// Dynamic shared memory of the separable kernel for one box's kinds.
-struct SepSmem {
-  int W[3];  // coarse window per direction
-  int P0;    // S0 row pitch (odd)
-  int s0, s1, s2; // sizes (doubles) of S0 (one buffer), S1, S2
-  size_t bytes() const { return sizeof(double) * (size_t)(2 * s0 + s1 + s2); }
-};
-
-SepSmem sep_smem_for(const int kind[3]);
-
 // Launchers (stream-ordered, no synchronisation).
-cudaError_t launch_sep_box(const BoxDesc &b, cudaStream_t s);
-cudaError_t launch_sep_level(const BoxDesc *d_boxes, const TileRef *d_tiles,
-                             int ntiles, int *d_counter, int s0max, int s1max,
-                             size_t smem_bytes, int grid, cudaStream_t s);
-int sep_level_grid(size_t smem_bytes);
+
+cudaError_t launch_stream_box(const BoxDesc &b, cudaStream_t s);
+// Level launch of the items of one z-window group (stream_zgroup of the
+// boxes' z kind); d_items holds only items of that group.
+cudaError_t launch_stream_level(int group, const BoxDesc *d_boxes,
+                                const TileRef *d_items, int nitems, int grid,
+                                cudaStream_t s);
+int stream_level_grid(int group);
+int stream_zgroup(int kz);
+constexpr int kStrGroups = 9;
+// Fills tbase/ntile/zchunk of a box for the streaming kernel.
+void stream_tiling(BoxDesc &b);
 
 cudaError_t launch_point_box(const BoxDesc &b, int per_group,
                              signed char *shifts, unsigned char *fallback,
