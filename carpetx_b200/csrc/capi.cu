@@ -161,6 +161,13 @@ int make_box(cx_op_t op, const double *crse, const int clo[3], const int chi[3],
   return CX_OK;
 }
 
+// The separable operators run on the streaming kernel (pair instantiation);
+// everything else on the pointwise kernel.
+bool use_stream(cx_op_t op, int per_group) {
+  return op_separable(op, per_group) &&
+         stream_pair_of(op_kind(op, 0), op_kind(op, 1), op_kind(op, 2)) >= 0;
+}
+
 int check_device() {
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
@@ -258,9 +265,9 @@ int cx_prolong_box_diag(cx_op_t op, const double *crse, const int crse_lo[3], co
   if (int e = check_device())
     return e;
   cudaStream_t s = (cudaStream_t)stream;
-  if (op_separable(op, per_group) && !shifts && !fallback)
+  if (use_stream(op, per_group) && !shifts && !fallback)
     return cuda_status(launch_stream_box(b, s), "prolongation launch");
-  if (op_separable(op, per_group)) {
+  if (use_stream(op, per_group)) {
     // diagnostics requested for an operator without shifts or fallback:
     // values from the separable kernel, diagnostics all zero
     const int64_t nreg = box_points(reg_lo, reg_hi) * (per_group ? 1 : ncomp);
@@ -313,14 +320,15 @@ int cx_level_plan_create(const cx_box_t *boxes, int nboxes, int per_group, cx_le
     p->bytes += 8 * (box_points(cl, ch) + box_points(x.reg_lo, x.reg_hi)) * x.ncomp;
     const int id = (int)p->boxes.size();
     p->boxes.push_back(b);
-    if (op_separable(x.op, per_group))
+    if (use_stream(x.op, per_group))
       sep_ids.push_back(id);
     else
       p->point_boxes.push_back(id);
   }
   // work items of the separable boxes: (box, x tile, y tile, z chunk,
-  // component), sorted by streamed planes, largest first; the kernel deals
-  // them round-robin to its persistent CTAs
+  // component), grouped by kernel instantiation and sorted by streamed
+  // planes, largest first; each kernel deals them round-robin to its
+  // persistent CTAs
   std::vector<std::pair<int, TileRef>> keyed;
   for (int id : sep_ids) {
     const BoxDesc &b = p->boxes[id];
@@ -336,7 +344,10 @@ int cx_level_plan_create(const cx_box_t *boxes, int nboxes, int per_group, cx_le
       }
   }
   // by z-window group (one kernel each), then by cost, largest first
-  auto group_of = [&](const TileRef &t) { return stream_zgroup(p->boxes[t.box].kind[2]); };
+  auto group_of = [&](const TileRef &t) {
+    const BoxDesc &b = p->boxes[t.box];
+    return stream_pair_of(b.kind[0], b.kind[1], b.kind[2]);
+  };
   std::stable_sort(keyed.begin(), keyed.end(),
                    [&](const std::pair<int, TileRef> &a, const std::pair<int, TileRef> &b) {
                      const int ga = group_of(a.second), gb = group_of(b.second);

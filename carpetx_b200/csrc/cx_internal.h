@@ -43,14 +43,16 @@ struct TileRef {
 // Launchers (stream-ordered, no synchronisation).
 
 cudaError_t launch_stream_box(const BoxDesc &b, cudaStream_t s);
-// Level launch of the items of one z-window group (stream_zgroup of the
-// boxes' z kind); d_items holds only items of that group.
-cudaError_t launch_stream_level(int group, const BoxDesc *d_boxes,
+// Streaming-kernel instantiation (stream_pairs.h) serving an operator's
+// kinds, -1 if none.
+int stream_pair_of(int kx, int ky, int kz);
+constexpr int kStrGroups = 17; // number of instantiations (kStreamPairs)
+// Level launch of the items of one instantiation; d_items holds only items
+// of boxes served by that pair.
+cudaError_t launch_stream_level(int pair, const BoxDesc *d_boxes,
                                 const TileRef *d_items, int nitems, int grid,
                                 cudaStream_t s);
-int stream_level_grid(int group);
-int stream_zgroup(int kz);
-constexpr int kStrGroups = 9;
+int stream_level_grid(int pair);
 // Fills tbase/ntile/zchunk of a box for the streaming kernel.
 void stream_tiling(BoxDesc &b);
 

@@ -1,0 +1,121 @@
+// Host side of the streaming kernel: pair lookup, tiling, launches.
+#include "stream_kernel.cuh"
+#include "stream_pairs.h"
+
+namespace cxb {
+namespace stream {
+KernelFn kernel_part0(int pair);
+KernelFn kernel_part1(int pair);
+KernelFn kernel_part2(int pair);
+KernelFn kernel_part3(int pair);
+
+namespace {
+KernelFn kernel_for(int pair) {
+  KernelFn k = kernel_part0(pair);
+  if (!k)
+    k = kernel_part1(pair);
+  if (!k)
+    k = kernel_part2(pair);
+  if (!k)
+    k = kernel_part3(pair);
+  return k;
+}
+
+int g_sms = 0;
+int g_grid[kStreamPairs] = {};
+
+int sms() {
+  if (!g_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  return g_sms;
+}
+} // namespace
+} // namespace stream
+
+int stream_pair_of(int kx, int ky, int kz) {
+  const int k[3] = {kx, ky, kz};
+  int v = -1, c = -1;
+  for (int d = 0; d < 3; ++d) {
+    if (kind_info(k[d]).cent == CC)
+      c = k[d];
+    else
+      v = k[d];
+  }
+  static const int pv[kStreamPairs] = {
+#define CXB_PV(I, V, C, KVI, KCI) KVI,
+      CXB_STREAM_PAIRS(CXB_PV)
+#undef CXB_PV
+  };
+  static const int pc[kStreamPairs] = {
+#define CXB_PC(I, V, C, KVI, KCI) KCI,
+      CXB_STREAM_PAIRS(CXB_PC)
+#undef CXB_PC
+  };
+  for (int i = 0; i < kStreamPairs; ++i)
+    if ((v < 0 || pv[i] == v) && (c < 0 || pc[i] == c))
+      return i;
+  return -1;
+}
+
+void stream_tiling(BoxDesc &b) {
+  const int T[2] = {stream::SX, stream::SY};
+  for (int d = 0; d < 3; ++d)
+    b.tbase[d] = b.rlo[d] & ~1;
+  for (int d = 0; d < 2; ++d)
+    b.ntile[d] = (b.rhi[d] - b.tbase[d] + T[d]) / T[d];
+  // fine z per item: whole columns up to 96 fine points, else near-equal
+  // even chunks of at most 96 (the z halo costs extra planes per chunk)
+  const int E = b.rhi[2] - b.tbase[2] + 1;
+  const int nch = (E + 95) / 96;
+  int zc = (E + nch - 1) / nch;
+  zc += zc & 1;
+  b.zchunk = zc;
+  b.ntile[2] = (E + zc - 1) / zc;
+}
+
+int stream_level_grid(int pair) {
+  using namespace stream;
+  if (pair < 0 || pair >= kStreamPairs)
+    return 0;
+  if (!g_grid[pair]) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel_for(pair), NTS, 0);
+    g_grid[pair] = sms() * (per_sm > 0 ? per_sm : 1);
+  }
+  return g_grid[pair];
+}
+
+cudaError_t launch_stream_box(const BoxDesc &b, cudaStream_t s) {
+  using namespace stream;
+  const int64_t n64 = (int64_t)b.ntile[0] * b.ntile[1] * b.ntile[2] * b.ncomp;
+  if (n64 <= 0)
+    return cudaSuccess;
+  if (n64 > INT32_MAX)
+    return cudaErrorInvalidValue;
+  const int pair = stream_pair_of(b.kind[0], b.kind[1], b.kind[2]);
+  KernelFn k = pair >= 0 ? kernel_for(pair) : nullptr;
+  if (!k)
+    return cudaErrorInvalidValue;
+  const int n = (int)n64;
+  const int cap = stream_level_grid(pair);
+  k<<<n < cap ? n : cap, NTS, 0, s>>>(b, nullptr, nullptr, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stream_level(int pair, const BoxDesc *d_boxes, const TileRef *d_items,
+                                int nitems, int grid, cudaStream_t s) {
+  using namespace stream;
+  if (nitems <= 0)
+    return cudaSuccess;
+  KernelFn k = kernel_for(pair);
+  if (!k)
+    return cudaErrorInvalidValue;
+  BoxDesc unused{};
+  k<<<grid < nitems ? grid : nitems, NTS, 0, s>>>(unused, d_boxes, d_items, nitems);
+  return cudaGetLastError();
+}
+
+} // namespace cxb
