@@ -338,9 +338,13 @@ int cx_level_plan_create(const cx_box_t *boxes, int nboxes, int per_group, cx_le
         const int z0 = b.tbase[2] + tz * b.zchunk;
         const int z1 = std::min(z0 + b.zchunk - 1, b.rhi[2]);
         const int planes = (z1 >> 1) - (z0 >> 1) + 1 + L;
-        for (int ty = 0; ty < b.ntile[1]; ++ty)
-          for (int tx = 0; tx < b.ntile[0]; ++tx)
-            keyed.push_back({planes, TileRef{id, (int16_t)tx, (int16_t)ty, (int16_t)tz, (int16_t)c}});
+        for (int tx = 0; tx < b.ntile[0]; ++tx) {
+          const int xb = b.tbase[0] + tx * b.xcw;
+          const int W = std::min(b.xcw, b.rhi[0] - xb + 1);
+          const int nub = (b.npr * W + b.upi - 1) / b.upi; // non-empty unit blocks
+          for (int ub = 0; ub < nub; ++ub)
+            keyed.push_back({planes, TileRef{id, (int16_t)tx, (int16_t)ub, (int16_t)tz, (int16_t)c}});
+        }
       }
   }
   // by z-window group (one kernel each), then by cost, largest first

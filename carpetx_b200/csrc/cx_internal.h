@@ -7,10 +7,11 @@
 
 namespace cxb {
 
-// Column of the streaming kernel: kStrX x kStrY fine points in x and y, fine
-// z in chunks of BoxDesc::zchunk; kStrFY fine y per thread.
-constexpr int kStrX = 32, kStrY = 16, kStrFY = 2;
-constexpr int kStrThreads = kStrX * kStrY / kStrFY;
+// Streaming kernel: threads per CTA = column units per work item; at most
+// kStrPairRows pairs of fine y rows and kStrMaxWidth fine x per item.
+constexpr int kStrThreads = 256;
+constexpr int kStrPairRows = 32;
+constexpr int kStrMaxWidth = 130;
 
 // One box of a transfer as the kernels see it.  Coordinates are AMReX index
 // space; strides in elements.
@@ -26,11 +27,14 @@ struct BoxDesc {
   int nlo[3], nhi[3]; // coarse points the operator reads (inclusive)
   int tbase[3];       // tile origin base: rlo rounded down to even (the
                       // tile origin is even, so fine offset = local & 1)
-  int ntile[3];       // tiles per direction (streaming kernel: x, y, z chunks)
+  int ntile[3];       // streaming kernel: x chunks, unit blocks, z chunks
   int kind[3];        // 1-D stencil kind per direction
   int op;             // operator handle
   int ncomp;
   int zchunk;         // streaming kernel: fine z per item (even)
+  int xcw;            // streaming kernel: fine x per x chunk
+  int npr;            // streaming kernel: pairs of fine y rows
+  int upi;            // streaming kernel: units (columns) per item
 };
 
 // One unit of work of the level kernel: a tile of a box, one component.

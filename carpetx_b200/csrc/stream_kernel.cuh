@@ -2,14 +2,17 @@
 // minmod), templated on the operator's pair of 1-D stencil kinds: KV for its
 // vertex-centred directions, KC for its cell-centred ones.
 //
-// A work item is one component of an SX x SY fine column of a box, over a
-// chunk of fine z.  The CTA streams the coarse z planes of the column's
-// window through a ring of shared-memory planes:
+// A work item is one component of a block of up to NU fine "units" of a box
+// over a chunk of fine z; a unit is a column (fine x, pair of fine y sharing
+// a coarse y centre), units are numbered x fastest over the box's x chunk
+// (any width up to WFMAX), so every lane works on a real fine point whatever
+// the box shape.  The CTA streams the coarse z planes of the block's window
+// through a ring of shared-memory planes:
 //   load    plane c + DPF of the coarse window (asynchronous 8-byte copies,
 //           zero-filled outside the coarse points the operator reads);
-//   x pass  X[cy][fx] = interp_x(coarse row), 4 fine x per thread from a
+//   x pass  X[cy][fx] = interp_x(coarse row), XB fine x per task from a
 //           register window, into shared memory;
-//   y pass  each thread computes Y[fy][fx] for its FYT fine y from a register
+//   y pass  each thread computes Y for its unit's 2 fine y from a register
 //           window of X (consecutive lanes = consecutive fine x);
 //   z pass  each thread keeps the Y values of the last L coarse planes in a
 //           register ring; once the ring holds the stencil of coarse centre
@@ -29,25 +32,43 @@
 namespace cxb {
 namespace stream {
 
-constexpr int SX = kStrX, SY = kStrY, FYT = kStrFY, NTS = kStrThreads;
-constexpr int DPF = 3;         // coarse planes prefetched ahead
-constexpr int NRING = DPF + 1; // shared-memory plane ring
-constexpr int MAXW = 8;        // largest RHI - RLO of a separable kind
-constexpr int MAXWX = SX / 2 + MAXW, MAXWY = SY / 2 + MAXW;
-constexpr int P0MAX = MAXWX | 1; // odd row pitch of a coarse plane
-constexpr int PLANE = P0MAX * MAXWY;
-constexpr int PX = SX + 1; // row pitch of the x-pass result
-constexpr int LDMAX = (PLANE + NTS - 1) / NTS;
-constexpr int XB = 4;                   // fine x per x-pass task
-constexpr int XSEG = SX / XB;           // x-pass tasks per row
-static_assert(SX == 32, "lanes map to fine x");
-static_assert(NTS == SX * SY / FYT, "one thread per (fine x, group of FYT fine y)");
-static_assert(FYT == 2, "the y pass emits 2 fine y per thread");
-static_assert(XSEG * 16 <= NTS && MAXWY <= 16, "x pass: 16 rows per segment");
+constexpr int NTS = kStrThreads; // threads per CTA = column units per item
+constexpr int NU = NTS;
+constexpr int FYT = 2;           // fine y per unit (one coarse y centre)
+constexpr int PRMAX = kStrPairRows; // pair rows per item at most
+constexpr int WFMAX = kStrMaxWidth; // fine x per x chunk at most
+constexpr int DPF = 3;           // coarse planes prefetched ahead
+constexpr int NRING = DPF + 1;   // shared-memory plane ring
+constexpr int MAXW = 8;          // largest RHI - RLO of a separable kind
+constexpr int XB = 4;            // fine x per x-pass task
+
+// Geometry of an item whose x chunk is W fine points wide (worst case over
+// the stencil kinds): rows of the coarse window / x-pass result, their
+// pitches, x-pass tasks.
+__host__ __device__ constexpr int span_rows(int W) {
+  return PRMAX < (NU - 1) / W + 2 ? PRMAX : (NU - 1) / W + 2;
+}
+__host__ __device__ constexpr int nseg_of(int W) { return (W + XB - 1) / XB; }
+__host__ __device__ constexpr int p0_of(int W, int wx) { return (nseg_of(W) * XB / 2 + wx) | 1; }
+__host__ __device__ constexpr int pxw_of(int W) { return (nseg_of(W) * XB) | 1; }
+__host__ __device__ constexpr int max_over_w(int what) {
+  int m = 0;
+  for (int W = 1; W <= WFMAX; ++W) {
+    const int nr = span_rows(W) + MAXW;
+    const int v = what == 0 ? nr * p0_of(W, MAXW) : what == 1 ? nr * pxw_of(W) : nr * nseg_of(W);
+    m = v > m ? v : m;
+  }
+  return m;
+}
+constexpr int PLANE = max_over_w(0); // coarse plane window (doubles)
+constexpr int XBUF = max_over_w(1);  // x-pass result (doubles)
+constexpr int LDMAX = (PLANE + NU - 1) / NU;
+constexpr int XTMAX = (max_over_w(2) + NU - 1) / NU;
+static_assert(NU % 32 == 0, "whole warps");
 
 struct Shared {
   double s0[NRING][PLANE];
-  double xs[MAXWY * PX];
+  double xs[XBUF];
 };
 
 __device__ __forceinline__ void cp_async8(double *sdst, const double *gsrc, int bytes) {
@@ -62,22 +83,14 @@ __device__ __forceinline__ void cp_async_wait_dpf() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(DPF) : "memory");
 }
 
-// x pass of one coarse plane: XB fine x per task; task = seg * 16 + row, so
-// a half warp covers 16 rows of one segment (odd pitches: conflict-free
-// 8-byte accesses).
+// One x-pass task: XB fine x from a register window of a coarse row.
 template <class K>
-__device__ __forceinline__ void xpass(const double *__restrict__ S0, int P0, int Wy,
-                                      double *__restrict__ xs) {
+__device__ __forceinline__ void xtask(const double *__restrict__ src, double *__restrict__ dst) {
   constexpr int WIN = XB / 2 + K::RHI - K::RLO;
-  const int seg = threadIdx.x >> 4, row = threadIdx.x & 15;
-  if (seg >= XSEG || row >= Wy)
-    return;
-  const double *src = S0 + row * P0 + seg * (XB / 2);
   double v[WIN];
 #pragma unroll
   for (int i = 0; i < WIN; ++i)
     v[i] = src[i];
-  double *dst = xs + row * PX + seg * XB;
 #pragma unroll
   for (int f = 0; f < XB; ++f) {
     if (f & 1)
@@ -87,38 +100,42 @@ __device__ __forceinline__ void xpass(const double *__restrict__ S0, int P0, int
   }
 }
 
-// y pass: the 2 fine y fy0, fy0+1 of this thread's fine x share the coarse
-// window starting at row fy0/2 of xs.
+// y pass of one unit: its 2 fine y share the coarse y window starting at
+// src (rows pxw apart).
 template <class K>
-__device__ __forceinline__ void ypass(const double *__restrict__ xs, int fy0, double y[2]) {
+__device__ __forceinline__ void ypass(const double *__restrict__ src, int pxw, double y[2]) {
   constexpr int W = 1 + K::RHI - K::RLO;
   double v[W];
-  const double *src = xs + (fy0 >> 1) * PX + (threadIdx.x & 31);
 #pragma unroll
   for (int i = 0; i < W; ++i)
-    v[i] = src[i * PX];
+    v[i] = src[i * pxw];
   y[0] = K::template ap<0>(v - K::RLO);
   y[1] = K::template ap<1>(v - K::RLO);
 }
 
-// Per-item geometry shared by all planes.
+// Per-item, per-thread geometry shared by all planes.
 struct Item {
   const double *cbase; // coarse component base
   int64_t cplane;      // coarse z-plane stride
   int clo_z, nlo_z, nhi_z;
   int c_first, c_last; // coarse planes streamed
-  int P0, Wy;
-  int ccx, ccy, ccz; // 1: the direction is cell centred (KC), 0: vertex (KV)
-  // this thread's fine column: address of (fx, fy0) at fz = 0; fy0 + 1 is
-  // fnx further; colmask bit j: fy0 + j inside the region
+  int pxw;             // row pitch of the x-pass result
+  int ccx, ccy, ccz;   // 1: the direction is cell centred (KC), 0: vertex (KV)
+  // this thread's unit: y window start in xs (-1: inactive unit); address of
+  // (fx, fy0) at fz = 0 (fy0 + 1 is fnx further); colmask bit j: fy0 + j
+  // inside the region
+  int ysrc;
   double *col;
   int fnx, colmask;
   int64_t fplane;
   int zlo, zhi; // fine z emitted (inclusive)
-  // this thread's share of a coarse plane load: smem offset (-1: none) and
-  // offset within the coarse z plane (-1: outside the read range in x or y)
+  // coarse plane loads: smem offset (-1: none) and offset within the coarse
+  // z plane (-1: outside the read range in x or y, zero-filled)
   int ld_soff[LDMAX];
   int ld_goff[LDMAX];
+  // x-pass tasks: smem offsets into the plane and into xs (-1: none)
+  int xt_src[XTMAX];
+  int xt_dst[XTMAX];
 };
 
 __device__ __forceinline__ void load_plane(const Item &it, int c, double *S0) {
@@ -145,7 +162,6 @@ template <class KV, class KC> __device__ __forceinline__ void stream_item(Shared
   constexpr int ZLO = PairInfo<KV, KC>::ZLO, ZHI = PairInfo<KV, KC>::ZHI;
   constexpr int L = ZHI - ZLO + 1;
   double ring[L][FYT];
-  const int fy0 = (threadIdx.x >> 5) * FYT;
 #pragma unroll
   for (int d = 0; d < DPF; ++d) {
     if (it.c_first + d <= it.c_last)
@@ -164,16 +180,23 @@ template <class KV, class KC> __device__ __forceinline__ void stream_item(Shared
     }
     cp_async_wait_dpf();
     __syncthreads();
-    if (it.ccx)
-      xpass<KC>(sh.s0[slot], it.P0, it.Wy, sh.xs);
-    else
-      xpass<KV>(sh.s0[slot], it.P0, it.Wy, sh.xs);
+#pragma unroll
+    for (int k = 0; k < XTMAX; ++k) {
+      if (it.xt_src[k] < 0)
+        continue;
+      if (it.ccx)
+        xtask<KC>(sh.s0[slot] + it.xt_src[k], sh.xs + it.xt_dst[k]);
+      else
+        xtask<KV>(sh.s0[slot] + it.xt_src[k], sh.xs + it.xt_dst[k]);
+    }
     __syncthreads();
-    double y[FYT];
-    if (it.ccy)
-      ypass<KC>(sh.xs, fy0, y);
-    else
-      ypass<KV>(sh.xs, fy0, y);
+    double y[FYT] = {0.0, 0.0};
+    if (it.ysrc >= 0) {
+      if (it.ccy)
+        ypass<KC>(sh.xs + it.ysrc, it.pxw, y);
+      else
+        ypass<KV>(sh.xs + it.ysrc, it.pxw, y);
+    }
 #pragma unroll
     for (int i = 0; i < L - 1; ++i)
 #pragma unroll
@@ -211,70 +234,102 @@ template <class KV, class KC> __device__ __forceinline__ void stream_item(Shared
   __syncthreads(); // the next item reuses the plane ring and xs
 }
 
-// Geometry of work item (tx, ty, chunk, comp) of box b; [zlo, zhi] is the
-// streaming window of the pair.
-__device__ __forceinline__ void make_item(const BoxDesc &b, int tx, int ty, int chunk, int comp,
-                                          int zwlo, int zwhi, Item &it) {
+// Geometry of work item (x chunk, unit block, z chunk, comp) of box b, for
+// the pair's streaming window [zwlo, zwhi] (union of the two z windows).
+// The item's units are the unit block's consecutive (pair row, fine x)
+// columns of the x chunk, flattened x fastest; thread t owns unit t.
+// Returns false if the block holds no unit (box mode, narrow last chunk).
+__device__ __forceinline__ bool make_item(const BoxDesc &b, int xchunk, int ublock, int zchunk,
+                                          int comp, int zwlo, int zwhi, Item &it) {
   const int kx = b.kind[0], ky = b.kind[1];
   it.ccx = kind_info(kx).cent;
   it.ccy = kind_info(ky).cent;
   it.ccz = kind_info(b.kind[2]).cent;
-  const int ox = b.tbase[0] + tx * SX, oy = b.tbase[1] + ty * SY;
-  const int oz = b.tbase[2] + chunk * b.zchunk;
+  const int xb = b.tbase[0] + xchunk * b.xcw;
+  const int W = min(b.xcw, b.rhi[0] - xb + 1);
+  const int nunits = b.npr * W;
+  const int u0 = ublock * b.upi;
+  if (u0 >= nunits)
+    return false;
+  const int uend = min(u0 + b.upi, nunits);
+  const int pr_lo = u0 / W, pr_hi = (uend - 1) / W;
   const int rlx = sep_rlo(kx), rly = sep_rlo(ky);
-  const int Wx = SX / 2 + sep_rhi(kx) - rlx;
-  it.Wy = SY / 2 + sep_rhi(ky) - rly;
-  it.P0 = Wx | 1;
-  const int cx0 = ox / 2 + rlx, cy0 = oy / 2 + rly;
+  const int NR = pr_hi - pr_lo + 1 + sep_rhi(ky) - rly;
+  const int nseg = nseg_of(W);
+  const int Wx = (W - 1) / 2 + 1 + sep_rhi(kx) - rlx;
+  const int P0 = p0_of(W, sep_rhi(kx) - rlx);
+  it.pxw = pxw_of(W);
+  const int cxb = xb / 2 + rlx;                   // xb even
+  const int cyb = b.tbase[1] / 2 + pr_lo + rly;   // tbase even
   it.cbase = b.crse + comp * b.cnp;
   it.cplane = (int64_t)b.cnx * b.cny;
   it.clo_z = b.clo[2];
   it.nlo_z = b.nlo[2];
   it.nhi_z = b.nhi[2];
+  const int oz = b.tbase[2] + zchunk * b.zchunk;
   const int zend = min(oz + b.zchunk - 1, b.rhi[2]);
   it.c_first = (oz >> 1) + zwlo;
   it.c_last = (zend >> 1) + zwhi;
   it.zlo = max(oz, b.rlo[2]);
   it.zhi = zend;
-  // fine column of this thread
-  const int fx = ox + (threadIdx.x & 31);
-  const int fyb = oy + (threadIdx.x >> 5) * FYT;
+  // this thread's unit
+  const int u = u0 + (int)threadIdx.x;
   it.fplane = (int64_t)b.fnx * b.fny;
   it.fnx = b.fnx;
-  const bool xok = fx >= b.rlo[0] && fx <= b.rhi[0];
   it.colmask = 0;
+  it.ysrc = -1;
+  it.col = b.fine;
+  if (u < uend) {
+    const int pr = u / W, fxl = u - pr * W;
+    const int fx = xb + fxl, fy0 = b.tbase[1] + 2 * pr;
+    it.ysrc = (pr - pr_lo) * it.pxw + fxl;
+    if (fx >= b.rlo[0]) {
 #pragma unroll
-  for (int j = 0; j < FYT; ++j) {
-    const int fy = fyb + j;
-    if (xok && fy >= b.rlo[1] && fy <= b.rhi[1])
-      it.colmask |= 1 << j;
+      for (int j = 0; j < FYT; ++j)
+        if (fy0 + j >= b.rlo[1] && fy0 + j <= b.rhi[1])
+          it.colmask |= 1 << j;
+    }
+    it.col = b.fine + comp * b.fnp + (fx - b.flo[0]) + (int64_t)b.fnx * (fy0 - b.flo[1]) -
+             it.fplane * b.flo[2];
   }
-  it.col = b.fine + comp * b.fnp + (fx - b.flo[0]) + (int64_t)b.fnx * (fyb - b.flo[1]) -
-           it.fplane * b.flo[2];
-  // this thread's elements of a coarse plane window
-  const int n = Wx * it.Wy;
+  // coarse plane window: NR rows x Wx columns
+  const int n = NR * Wx;
 #pragma unroll
   for (int i = 0; i < LDMAX; ++i) {
-    const int e = threadIdx.x + i * NTS;
-    if (e >= n) {
-      it.ld_soff[i] = -1;
-      it.ld_goff[i] = -1;
-      continue;
+    const int e = threadIdx.x + i * NU;
+    it.ld_soff[i] = -1;
+    it.ld_goff[i] = -1;
+    if (e < n) {
+      const int y = e / Wx, x = e - y * Wx;
+      it.ld_soff[i] = y * P0 + x;
+      const int gx = cxb + x, gy = cyb + y;
+      if (gx >= b.nlo[0] && gx <= b.nhi[0] && gy >= b.nlo[1] && gy <= b.nhi[1])
+        it.ld_goff[i] = (gy - b.clo[1]) * b.cnx + (gx - b.clo[0]);
     }
-    const int x = e % Wx, y = e / Wx;
-    it.ld_soff[i] = y * it.P0 + x;
-    const int gx = cx0 + x, gy = cy0 + y;
-    const bool ok = gx >= b.nlo[0] && gx <= b.nhi[0] && gy >= b.nlo[1] && gy <= b.nhi[1];
-    it.ld_goff[i] = ok ? (gy - b.clo[1]) * b.cnx + (gx - b.clo[0]) : -1;
   }
+  // x-pass tasks: NR rows x nseg segments, rows fastest
+  const int nt = NR * nseg;
+#pragma unroll
+  for (int k = 0; k < XTMAX; ++k) {
+    const int t = threadIdx.x + k * NU;
+    it.xt_src[k] = -1;
+    it.xt_dst[k] = -1;
+    if (t < nt) {
+      const int sg = t / NR, r = t - sg * NR;
+      it.xt_src[k] = r * P0 + sg * (XB / 2);
+      it.xt_dst[k] = r * it.pxw + sg * XB;
+    }
+  }
+  return true;
 }
 
 template <class KV, class KC>
-__device__ __forceinline__ void run_item(Shared &sh, const BoxDesc &b, int tx, int ty, int chunk,
-                                         int comp) {
+__device__ __forceinline__ void run_item(Shared &sh, const BoxDesc &b, int xchunk, int ublock,
+                                         int zchunk, int comp) {
   Item it;
-  make_item(b, tx, ty, chunk, comp, PairInfo<KV, KC>::ZLO, PairInfo<KV, KC>::ZHI, it);
-  stream_item<KV, KC>(sh, it);
+  // uniform over the CTA: an empty block is skipped by every thread
+  if (make_item(b, xchunk, ublock, zchunk, comp, PairInfo<KV, KC>::ZLO, PairInfo<KV, KC>::ZHI, it))
+    stream_item<KV, KC>(sh, it);
 }
 
 constexpr int BOX_WORDS = (int)(sizeof(BoxDesc) / sizeof(int));
@@ -293,13 +348,13 @@ __global__ void __launch_bounds__(NTS, 2)
   __shared__ BoxDesc box_s;
   if (!items) {
     for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-      const int tx = item % b.ntile[0];
+      const int xchunk = item % b.ntile[0];
       int r = item / b.ntile[0];
-      const int ty = r % b.ntile[1];
+      const int ublock = r % b.ntile[1];
       r /= b.ntile[1];
-      const int chunk = r % b.ntile[2];
+      const int zchunk = r % b.ntile[2];
       const int comp = r / b.ntile[2];
-      run_item<KV, KC>(sh, b, tx, ty, chunk, comp);
+      run_item<KV, KC>(sh, b, xchunk, ublock, zchunk, comp);
     }
     return;
   }

@@ -61,11 +61,24 @@ int stream_pair_of(int kx, int ky, int kz) {
 }
 
 void stream_tiling(BoxDesc &b) {
-  const int T[2] = {stream::SX, stream::SY};
+  using namespace stream;
   for (int d = 0; d < 3; ++d)
     b.tbase[d] = b.rlo[d] & ~1;
-  for (int d = 0; d < 2; ++d)
-    b.ntile[d] = (b.rhi[d] - b.tbase[d] + T[d]) / T[d];
+  // x chunks: the whole width up to WFMAX, else near-equal even chunks
+  const int Wt = b.rhi[0] - b.tbase[0] + 1;
+  if (Wt <= WFMAX) {
+    b.xcw = Wt;
+    b.ntile[0] = 1;
+  } else {
+    const int n = (Wt + WFMAX - 3) / (WFMAX - 2);
+    int w = (Wt + n - 1) / n;
+    w += w & 1;
+    b.xcw = w;
+    b.ntile[0] = (Wt + w - 1) / w;
+  }
+  b.npr = (b.rhi[1] - b.tbase[1]) / 2 + 1;
+  b.upi = NU < PRMAX * b.xcw ? NU : PRMAX * b.xcw;
+  b.ntile[1] = (b.npr * b.xcw + b.upi - 1) / b.upi;
   // fine z per item: whole columns up to 96 fine points, else near-equal
   // even chunks of at most 96 (the z halo costs extra planes per chunk)
   const int E = b.rhi[2] - b.tbase[2] + 1;
