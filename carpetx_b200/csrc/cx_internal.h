@@ -7,10 +7,11 @@
 
 namespace cxb {
 
-// Streaming kernel: threads per CTA = column units per work item; at most
+// Streaming kernel: threads per CTA, column units per thread; at most
 // kStrPairRows pairs of fine y rows and kStrMaxWidth fine x per item.
 constexpr int kStrThreads = 256;
-constexpr int kStrPairRows = 32;
+constexpr int kStrUnitsPerThread = 2;
+constexpr int kStrPairRows = 64;
 constexpr int kStrMaxWidth = 130;
 
 // One box of a transfer as the kernels see it.  Coordinates are AMReX index

@@ -3,9 +3,13 @@
 // Each struct applies the reference's interp1d<...> (CarpetX/src/
 // prolongate_3d_rf2_impl.hxx:396-878) with the reference's association order,
 // every product and sum rounded separately (__dmul_rn / __dadd_rn: no FMA
-// contraction), so that results are bit-identical to the host build of the
-// reference.  `v` points at the value of coarse offset 0 of the fine point;
-// OFF is the fine point's offset within its coarse cell.
+// contraction), so that results equal the host build of the reference as FP64
+// values.  Two exact simplifications: the reference starts its sums from
+// y = 0 and adds the first product (0 + p = p, except that 0 + (-0) = +0), and
+// multiplies by the coefficient 1 (exact); both are skipped, so only the sign
+// of an exact-zero result can differ.  `v` points at the value of coarse
+// offset 0 of the fine point; OFF is the fine point's offset within its
+// coarse cell.
 //   RLO/RHI: union over OFF of the stencil radius (window the passes stage).
 #pragma once
 #include "cx_kinds.h"
@@ -47,9 +51,9 @@ template <int P> struct VcPoly {
       return v[0];
     } else {
       constexpr int N = P + 1, i0 = N / 2 - 1;
-      double y = 0.0;
+      double y = fmul(vc_poly_c<P>(0), fadd(v[-i0], v[P - i0]));
 #pragma unroll
-      for (int i = 0; i < N / 2; ++i)
+      for (int i = 1; i < N / 2; ++i)
         y = fadd(y, fmul(vc_poly_c<P>(i), fadd(v[i - i0], v[P - i - i0])));
       return y;
     }
@@ -62,9 +66,9 @@ template <int P> struct CcPoly {
   static constexpr int N = P + 1, I0 = N / 2;
   static constexpr int RLO = -I0, RHI = N - 1 - I0 + P % 2;
   template <int OFF> __device__ __forceinline__ static double ap(const double *v) {
-    double y = 0.0;
+    double y = OFF == 0 ? fmul(cc_poly_c<P>(0), v[-I0]) : fmul(cc_poly_c<P>(P), v[-I0 + P % 2]);
 #pragma unroll
-    for (int i = 0; i < N; ++i) {
+    for (int i = 1; i < N; ++i) {
       if constexpr (OFF == 0)
         y = fadd(y, fmul(cc_poly_c<P>(i), v[i - I0]));
       else
@@ -83,7 +87,8 @@ template <int P> struct CcCons {
   template <int OFF> __device__ __forceinline__ static double ap(const double *v) {
     double y;
     if constexpr (P % 2 == 0) {
-      y = fmul(cc_cons_c<P>(P / 2), v[P / 2 - I0]);
+      static_assert(cc_cons_c<P>(P / 2) == 1.0, "even conservative stencils have centre weight 1");
+      y = v[P / 2 - I0];
 #pragma unroll
       for (int i = 0; i < P / 2; ++i) {
         if constexpr (OFF == 0)
@@ -92,9 +97,9 @@ template <int P> struct CcCons {
           y = fadd(y, fmul(cc_cons_c<P>(i), fsub(v[P - i - I0], v[i - I0])));
       }
     } else {
-      y = 0.0;
+      y = OFF == 0 ? fmul(cc_cons_c<P>(0), v[-I0]) : fmul(cc_cons_c<P>(0), v[(P + 1) / 2]);
 #pragma unroll
-      for (int i = 0; i < N; ++i) {
+      for (int i = 1; i < N; ++i) {
         if constexpr (OFF == 0)
           y = fadd(y, fmul(cc_cons_c<P>(i), v[i - I0]));
         else
@@ -112,11 +117,11 @@ template <int P> struct VcCons {
   static constexpr int RLO = 0, RHI = P == 0 ? 0 : 1;
   template <int OFF> __device__ __forceinline__ static double ap(const double *v) {
     if constexpr (OFF == 0) {
-      return fadd(0.0, fmul(1.0, v[0]));
+      return v[0];
     } else if constexpr (P == 0) {
       return 0.0;
     } else {
-      return fadd(fadd(0.0, fmul(0.5, v[0])), fmul(0.5, v[1]));
+      return fadd(fmul(0.5, v[0]), fmul(0.5, v[1]));
     }
   }
 };
@@ -133,9 +138,9 @@ struct CcMinmod {
     // cval + sign * delta with sign = -1 (off 0) or +1 (off 1); the product
     // by +-1 is exact
     if constexpr (OFF == 0)
-      return fadd(cval, fmul(-1.0, delta));
+      return fsub(cval, delta);
     else
-      return fadd(cval, fmul(1.0, delta));
+      return fadd(cval, delta);
   }
 };
 

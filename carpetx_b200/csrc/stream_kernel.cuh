@@ -12,8 +12,9 @@
 //           zero-filled outside the coarse points the operator reads);
 //   x pass  X[cy][fx] = interp_x(coarse row), XB fine x per task from a
 //           register window, into shared memory;
-//   y pass  each thread computes Y for its unit's 2 fine y from a register
-//           window of X (consecutive lanes = consecutive fine x);
+//   y pass  each thread computes Y for the 2 fine y of each of its UPT
+//           units from a register window of X (consecutive lanes =
+//           consecutive fine x);
 //   z pass  each thread keeps the Y values of the last L coarse planes in a
 //           register ring; once the ring holds the stencil of coarse centre
 //           cc it emits fine z = 2cc and 2cc+1 straight to global memory.
@@ -32,8 +33,9 @@
 namespace cxb {
 namespace stream {
 
-constexpr int NTS = kStrThreads; // threads per CTA = column units per item
-constexpr int NU = NTS;
+constexpr int NTS = kStrThreads; // threads per CTA
+constexpr int UPT = kStrUnitsPerThread; // column units per thread
+constexpr int NU = NTS * UPT;    // column units per item
 constexpr int FYT = 2;           // fine y per unit (one coarse y centre)
 constexpr int PRMAX = kStrPairRows; // pair rows per item at most
 constexpr int WFMAX = kStrMaxWidth; // fine x per x chunk at most
@@ -62,8 +64,8 @@ __host__ __device__ constexpr int max_over_w(int what) {
 }
 constexpr int PLANE = max_over_w(0); // coarse plane window (doubles)
 constexpr int XBUF = max_over_w(1);  // x-pass result (doubles)
-constexpr int LDMAX = (PLANE + NU - 1) / NU;
-constexpr int XTMAX = (max_over_w(2) + NU - 1) / NU;
+constexpr int LDMAX = (PLANE + NTS - 1) / NTS;
+constexpr int XTMAX = (max_over_w(2) + NTS - 1) / NTS;
 static_assert(NU % 32 == 0, "whole warps");
 
 struct Shared {
@@ -121,12 +123,13 @@ struct Item {
   int c_first, c_last; // coarse planes streamed
   int pxw;             // row pitch of the x-pass result
   int ccx, ccy, ccz;   // 1: the direction is cell centred (KC), 0: vertex (KV)
-  // this thread's unit: y window start in xs (-1: inactive unit); address of
-  // (fx, fy0) at fz = 0 (fy0 + 1 is fnx further); colmask bit j: fy0 + j
-  // inside the region
-  int ysrc;
-  double *col;
-  int fnx, colmask;
+  // this thread's units (tid and tid + NTS of the block): y window start in
+  // xs (-1: inactive unit); address of (fx, fy0) at fz = 0 (fy0 + 1 is fnx
+  // further); colmask bit j: fy0 + j inside the region
+  int ysrc[UPT];
+  double *col[UPT];
+  int colmask[UPT];
+  int fnx;
   int64_t fplane;
   int zlo, zhi; // fine z emitted (inclusive)
   // coarse plane loads: smem offset (-1: none) and offset within the coarse
@@ -161,7 +164,7 @@ template <class KV, class KC> struct PairInfo {
 template <class KV, class KC> __device__ __forceinline__ void stream_item(Shared &sh, const Item &it) {
   constexpr int ZLO = PairInfo<KV, KC>::ZLO, ZHI = PairInfo<KV, KC>::ZHI;
   constexpr int L = ZHI - ZLO + 1;
-  double ring[L][FYT];
+  double ring[L][UPT][FYT];
 #pragma unroll
   for (int d = 0; d < DPF; ++d) {
     if (it.c_first + d <= it.c_last)
@@ -190,21 +193,26 @@ template <class KV, class KC> __device__ __forceinline__ void stream_item(Shared
         xtask<KV>(sh.s0[slot] + it.xt_src[k], sh.xs + it.xt_dst[k]);
     }
     __syncthreads();
-    double y[FYT] = {0.0, 0.0};
-    if (it.ysrc >= 0) {
-      if (it.ccy)
-        ypass<KC>(sh.xs + it.ysrc, it.pxw, y);
-      else
-        ypass<KV>(sh.xs + it.ysrc, it.pxw, y);
-    }
 #pragma unroll
     for (int i = 0; i < L - 1; ++i)
 #pragma unroll
-      for (int j = 0; j < FYT; ++j)
-        ring[i][j] = ring[i + 1][j];
+      for (int q = 0; q < UPT; ++q)
 #pragma unroll
-    for (int j = 0; j < FYT; ++j)
-      ring[L - 1][j] = y[j];
+        for (int j = 0; j < FYT; ++j)
+          ring[i][q][j] = ring[i + 1][q][j];
+#pragma unroll
+    for (int q = 0; q < UPT; ++q) {
+      double y[FYT] = {0.0, 0.0};
+      if (it.ysrc[q] >= 0) {
+        if (it.ccy)
+          ypass<KC>(sh.xs + it.ysrc[q], it.pxw, y);
+        else
+          ypass<KV>(sh.xs + it.ysrc[q], it.pxw, y);
+      }
+#pragma unroll
+      for (int j = 0; j < FYT; ++j)
+        ring[L - 1][q][j] = y[j];
+    }
     if (c - it.c_first >= L - 1) {
       const int cc = c - ZHI; // coarse centre whose stencil is complete
 #pragma unroll
@@ -213,19 +221,21 @@ template <class KV, class KC> __device__ __forceinline__ void stream_item(Shared
         if (fz < it.zlo || fz > it.zhi)
           continue;
 #pragma unroll
-        for (int j = 0; j < FYT; ++j) {
-          double v[L];
+        for (int q = 0; q < UPT; ++q)
 #pragma unroll
-          for (int i = 0; i < L; ++i)
-            v[i] = ring[i][j];
-          double r;
-          if (it.ccz)
-            r = off ? KC::template ap<1>(v - ZLO) : KC::template ap<0>(v - ZLO);
-          else
-            r = off ? KV::template ap<1>(v - ZLO) : KV::template ap<0>(v - ZLO);
-          if (it.colmask & (1 << j))
-            __stcs(it.col + j * it.fnx + (int64_t)fz * it.fplane, r);
-        }
+          for (int j = 0; j < FYT; ++j) {
+            double v[L];
+#pragma unroll
+            for (int i = 0; i < L; ++i)
+              v[i] = ring[i][q][j];
+            double r;
+            if (it.ccz)
+              r = off ? KC::template ap<1>(v - ZLO) : KC::template ap<0>(v - ZLO);
+            else
+              r = off ? KV::template ap<1>(v - ZLO) : KV::template ap<0>(v - ZLO);
+            if (it.colmask[q] & (1 << j))
+              __stcs(it.col[q] + j * it.fnx + (int64_t)fz * it.fplane, r);
+          }
       }
     }
     if (++slot == NRING)
@@ -272,31 +282,34 @@ __device__ __forceinline__ bool make_item(const BoxDesc &b, int xchunk, int ublo
   it.c_last = (zend >> 1) + zwhi;
   it.zlo = max(oz, b.rlo[2]);
   it.zhi = zend;
-  // this thread's unit
-  const int u = u0 + (int)threadIdx.x;
+  // this thread's units
   it.fplane = (int64_t)b.fnx * b.fny;
   it.fnx = b.fnx;
-  it.colmask = 0;
-  it.ysrc = -1;
-  it.col = b.fine;
-  if (u < uend) {
-    const int pr = u / W, fxl = u - pr * W;
-    const int fx = xb + fxl, fy0 = b.tbase[1] + 2 * pr;
-    it.ysrc = (pr - pr_lo) * it.pxw + fxl;
-    if (fx >= b.rlo[0]) {
 #pragma unroll
-      for (int j = 0; j < FYT; ++j)
-        if (fy0 + j >= b.rlo[1] && fy0 + j <= b.rhi[1])
-          it.colmask |= 1 << j;
+  for (int q = 0; q < UPT; ++q) {
+    const int u = u0 + (int)threadIdx.x + q * NTS;
+    it.colmask[q] = 0;
+    it.ysrc[q] = -1;
+    it.col[q] = b.fine;
+    if (u < uend) {
+      const int pr = u / W, fxl = u - pr * W;
+      const int fx = xb + fxl, fy0 = b.tbase[1] + 2 * pr;
+      it.ysrc[q] = (pr - pr_lo) * it.pxw + fxl;
+      if (fx >= b.rlo[0]) {
+#pragma unroll
+        for (int j = 0; j < FYT; ++j)
+          if (fy0 + j >= b.rlo[1] && fy0 + j <= b.rhi[1])
+            it.colmask[q] |= 1 << j;
+      }
+      it.col[q] = b.fine + comp * b.fnp + (fx - b.flo[0]) + (int64_t)b.fnx * (fy0 - b.flo[1]) -
+                  it.fplane * b.flo[2];
     }
-    it.col = b.fine + comp * b.fnp + (fx - b.flo[0]) + (int64_t)b.fnx * (fy0 - b.flo[1]) -
-             it.fplane * b.flo[2];
   }
   // coarse plane window: NR rows x Wx columns
   const int n = NR * Wx;
 #pragma unroll
   for (int i = 0; i < LDMAX; ++i) {
-    const int e = threadIdx.x + i * NU;
+    const int e = threadIdx.x + i * NTS;
     it.ld_soff[i] = -1;
     it.ld_goff[i] = -1;
     if (e < n) {
@@ -311,7 +324,7 @@ __device__ __forceinline__ bool make_item(const BoxDesc &b, int xchunk, int ublo
   const int nt = NR * nseg;
 #pragma unroll
   for (int k = 0; k < XTMAX; ++k) {
-    const int t = threadIdx.x + k * NU;
+    const int t = threadIdx.x + k * NTS;
     it.xt_src[k] = -1;
     it.xt_dst[k] = -1;
     if (t < nt) {
@@ -340,8 +353,10 @@ static_assert(BOX_WORDS <= NTS, "one thread per descriptor word");
 // list (sorted by cost, largest first) dealt round-robin to persistent CTAs;
 // the descriptors of the next item are loaded into registers while the
 // current item streams, so no global-memory latency sits between two items.
+// Two CTAs per SM (at most 128 registers), except the order-7 pairs whose
+// register ring (9 planes) needs more: one CTA per SM.
 template <class KV, class KC>
-__global__ void __launch_bounds__(NTS, 2)
+__global__ void __launch_bounds__(NTS, PairInfo<KV, KC>::ZHI - PairInfo<KV, KC>::ZLO >= 8 ? 1 : 2)
     stream_kernel(const BoxDesc b, const BoxDesc *__restrict__ boxes,
                   const TileRef *__restrict__ items, int nitems) {
   __shared__ Shared sh;
