@@ -156,7 +156,7 @@ int make_box(cx_op_t op, const double *crse, const int clo[3], const int chi[3],
   b->fnx = fhi[0] - flo[0] + 1;
   b->fny = fhi[1] - flo[1] + 1;
   b->fnp = (int64_t)b->fnx * b->fny * (fhi[2] - flo[2] + 1);
-  stream_tiling(*b);
+  stream_tiling(*b, 0);
   (void)per_group;
   return CX_OK;
 }
@@ -265,6 +265,8 @@ int cx_prolong_box_diag(cx_op_t op, const double *crse, const int crse_lo[3], co
   if (int e = check_device())
     return e;
   cudaStream_t s = (cudaStream_t)stream;
+  if (use_stream(op, per_group)) // one box per launch: spread it over the GPU
+    stream_tiling(b, stream_level_grid(stream_pair_of(b.kind[0], b.kind[1], b.kind[2])));
   if (use_stream(op, per_group) && !shifts && !fallback)
     return cuda_status(launch_stream_box(b, s), "prolongation launch");
   if (use_stream(op, per_group)) {

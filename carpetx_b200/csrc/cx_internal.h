@@ -58,8 +58,10 @@ cudaError_t launch_stream_level(int pair, const BoxDesc *d_boxes,
                                 const TileRef *d_items, int nitems, int grid,
                                 cudaStream_t s);
 int stream_level_grid(int pair);
-// Fills tbase/ntile/zchunk of a box for the streaming kernel.
-void stream_tiling(BoxDesc &b);
+// Fills the streaming-kernel tiling of a box (tbase, ntile, zchunk, xcw,
+// npr, upi); min_items > 0 shortens the z chunks of a box launched alone so
+// that it spreads over at least that many CTAs where it can.
+void stream_tiling(BoxDesc &b, int min_items);
 
 cudaError_t launch_point_box(const BoxDesc &b, int per_group,
                              signed char *shifts, unsigned char *fallback,

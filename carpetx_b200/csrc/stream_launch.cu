@@ -60,7 +60,7 @@ int stream_pair_of(int kx, int ky, int kz) {
   return -1;
 }
 
-void stream_tiling(BoxDesc &b) {
+void stream_tiling(BoxDesc &b, int min_items) {
   using namespace stream;
   for (int d = 0; d < 3; ++d)
     b.tbase[d] = b.rlo[d] & ~1;
@@ -80,9 +80,14 @@ void stream_tiling(BoxDesc &b) {
   b.upi = NU < PRMAX * b.xcw ? NU : PRMAX * b.xcw;
   b.ntile[1] = (b.npr * b.xcw + b.upi - 1) / b.upi;
   // fine z per item: whole columns up to 96 fine points, else near-equal
-  // even chunks of at most 96 (the z halo costs extra planes per chunk)
+  // even chunks of at most 96 (the z halo costs extra planes per chunk);
+  // shorter chunks (down to 16) when the box alone must fill min_items CTAs
   const int E = b.rhi[2] - b.tbase[2] + 1;
-  const int nch = (E + 95) / 96;
+  const int64_t xy_items = (int64_t)b.ntile[0] * b.ntile[1] * b.ncomp;
+  int maxz = 96;
+  while (maxz > 16 && xy_items * ((E + maxz - 1) / maxz) < min_items)
+    maxz /= 2;
+  const int nch = (E + maxz - 1) / maxz;
   int zc = (E + nch - 1) / nch;
   zc += zc & 1;
   b.zchunk = zc;
