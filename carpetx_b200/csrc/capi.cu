@@ -523,3 +523,14 @@ int cx_prolong_adjoint_box(cx_op_t op, const double *crse, const int crse_lo[3],
 }
 
 } // extern "C"
+
+// Internal entry points for the allocation-free level transfer (noalloc.cu):
+// the same validation and dispatch rules as the entry points above.
+namespace cxb {
+int validate_box_for_level(const cx_box_t &x, int per_group, BoxDesc *b, bool *empty) {
+  return make_box(x.op, x.crse, x.crse_lo, x.crse_hi, x.fine, x.fine_lo, x.fine_hi, x.reg_lo,
+                  x.reg_hi, x.ncomp, per_group, b, empty);
+}
+bool box_uses_stream(cx_op_t op, int per_group) { return use_stream(op, per_group); }
+int record_failure(int status, const char *what) { return fail(status, "%s", what); }
+} // namespace cxb

@@ -138,6 +138,32 @@ int cx_level_plan_stats(cx_level_plan_t plan, int64_t *ntiles,
 int cx_level_plan_destroy(cx_level_plan_t plan);
 
 /* ---------------------------------------------------------------------- */
+/* A whole level without allocating device memory                          */
+
+/* Upper limits of cx_level_execute_noalloc: boxes per call, work items per
+ * call (an item is one component of up to 512 fine columns of a box over a
+ * chunk of at most 96 fine z points). */
+#define CX_NOALLOC_MAX_BOXES 1024
+#define CX_NOALLOC_MAX_ITEMS 131072
+
+/* The level transfer of cx_level_plan_create + cx_level_plan_execute, for
+ * callers that cannot allocate device memory: there is no plan object; the
+ * work list lives in one fixed device array of the library (about 1.7 MB per
+ * GPU, held until the process exits) and is rebuilt and copied onto `stream`
+ * at every call.  Allocates nothing: no cudaMalloc, no cudaFree, no
+ * allocating library call (an argument error records its message as every
+ * entry point does).  The first call on a device looks the array's address
+ * up (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  All calls share the one array and a call
+ * overwrites what the previous one left there, so calls whose kernels can
+ * overlap on the GPU (different streams without ordering between them) race;
+ * calls on one stream are ordered.  CX_EINVAL beyond CX_NOALLOC_MAX_BOXES
+ * boxes or CX_NOALLOC_MAX_ITEMS work items.  No counterpart in the reference
+ * (its operators never allocate device work lists). */
+int cx_level_execute_noalloc(const cx_box_t *boxes, int nboxes, int per_group,
+                             cx_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
 /* Restriction                                                             */
 
 /* Replaces the average_down family called by Restrict
