@@ -7,6 +7,11 @@ VVC, VCC; VVV boxes use "interpolate" order 5, the staggered ones "hermite"
 order 3.  Synthetic data (seeded normal values; the operators are linear, the
 values do not change the work).
 
+With N ranks (one per GPU, launched by torchrun) the level has 512 x N boxes,
+distributed over the ranks by the knapsack mapping of
+carpetx_b200.distribute; every rank transfers the boxes it owns (weak
+scaling, no data-path collective) and the time is the slowest rank's.
+
 One step = prolongation of every box and component of the level.  Reported:
   value      fine points/s of the batched transfer (one persistent launch,
              replayed from a CUDA graph), inputs resident in HBM
@@ -41,6 +46,9 @@ sys.path.insert(0, ROOT)
 METRIC = "FP64 fine points/s, batched persistent level prolongation"
 UNIT = "fine points/s"
 L2_BYTES = 126 * 1024 * 1024
+# ncu DRAM bytes per fine point of the level512 workload (both kernels of a
+# step, 2-component capture: 1551.8 MB for 172,696,778 fine points)
+TRAFFIC_PER_FINE_POINT = 1551.8e6 / 172696778
 
 
 def parse():
@@ -258,9 +266,15 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
-    # weak scaling: every rank transfers its own level (seed + rank); the
-    # boxes are independent, so there is no data-path collective
-    boxes, cfg = workload(args.workload, args.seed + rank, args.boxes, args.ncomp)
+    # weak scaling: one level of `boxes` x N boxes, knapsack-distributed over
+    # the N ranks (every rank computes the same mapping); a box's transfer is
+    # local to its owner, so there is no data-path collective
+    from carpetx_b200.distribute import box_cost, max_over_ranks as _max_over_ranks, my_boxes
+    from carpetx_b200.distribute import sum_over_ranks
+    all_boxes, cfg = workload(args.workload, args.seed, args.boxes * world, args.ncomp)
+    costs = [box_cost(b[5], b[6], b[7]) for b in all_boxes]
+    boxes = my_boxes(all_boxes, costs, rank, world)
+    total_fine = sum(costs)  # regions are the whole fine boxes
     coff, foff, ctot, ftot = [], [], 0, 0
     for b in boxes:
         coff.append(ctot)
@@ -303,11 +317,7 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return t.item()
+        return _max_over_ranks(x, dev)
 
     clocks = ClockSampler(local)
     barrier()
@@ -324,7 +334,7 @@ def main():
     per_step = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
     ms_total = max_over_ranks(ev[0].elapsed_time(ev[-1]))
     ms_step = ms_total / args.steps
-    value = world * nfine * args.steps / (ms_total / 1e3)
+    value = total_fine * args.steps / (ms_total / 1e3)
 
     # the same work launched once per box per component (our kernel)
     L = cb.lib()
@@ -360,7 +370,7 @@ def main():
         e1.record(stream)
         barrier()
         ms_pb = max_over_ranks(e0.elapsed_time(e1)) / args.per_box_steps
-        per_box_value = world * nfine / (ms_pb / 1e3)
+        per_box_value = total_fine / (ms_pb / 1e3)
 
     # end to end through the C ABI with host buffers
     ms_e2e, e2e_value = None, None
@@ -378,10 +388,15 @@ def main():
         e1.record(stream)
         barrier()
         ms_e2e = max_over_ranks(e0.elapsed_time(e1)) / args.e2e_steps
-        e2e_value = world * nfine / (ms_e2e / 1e3)
+        e2e_value = total_fine / (ms_e2e / 1e3)
 
     peak, peak_src = measured_peaks()
-    achieved = alg_bytes / (ms_step / 1e3) / 1e9
+    # per GPU: the ranks' mean algorithmic bytes over the slowest rank's time
+    mean_bytes = sum_over_ranks(alg_bytes, dev) / world
+    achieved = mean_bytes / (ms_step / 1e3) / 1e9
+    # DRAM traffic grows with the fine points: the measured bytes per point
+    # scaled to this step
+    traffic = (TRAFFIC_PER_FINE_POINT * nfine if args.workload == "level512" else None)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
@@ -389,7 +404,9 @@ def main():
         "config": dict(cfg, fine_points_per_gpu=nfine, algorithmic_bytes_per_gpu=alg_bytes,
                        l2_flush=f"inputs+outputs {(8 * (ctot + ftot)) / 1e9:.1f} GB per GPU "
                                 f">> L2 ({L2_BYTES / 2**20:.0f} MiB); no explicit flush",
-                       parallelism=f"weak: one independent level per GPU x{world}",
+                       boxes_total=len(all_boxes), boxes_this_rank=len(boxes),
+                       parallelism=f"weak: one level of {len(all_boxes)} boxes, knapsack-"
+                                   f"distributed over {world} rank(s), no data-path collective",
                        launch="one persistent kernel per step, CUDA graph replay"),
         "gpu_launches": args.steps,
         "per_box": {"value": per_box_value, "unit": UNIT, "ms_per_step": ms_pb,
@@ -398,7 +415,8 @@ def main():
         "e2e": {"value": e2e_value, "unit": UNIT, "ms_per_step": ms_e2e,
                 "h2d_bytes_per_step": 8 * ctot, "d2h_bytes_per_step": 8 * ftot},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": traffic,
+                     "traffic_unit": "bytes per step (rank 0)",
                      "peak_source": peak_src,
                      "frac_of_8TBs_spec": achieved / 8000.0,
                      "step_ms_min": min(per_step), "step_ms_max": max(per_step)},

@@ -359,7 +359,8 @@ template <class KV, class KC>
 __global__ void __launch_bounds__(NTS, PairInfo<KV, KC>::ZHI - PairInfo<KV, KC>::ZLO >= 8 ? 1 : 2)
     stream_kernel(const BoxDesc b, const BoxDesc *__restrict__ boxes,
                   const TileRef *__restrict__ items, int nitems) {
-  __shared__ Shared sh;
+  extern __shared__ __align__(16) unsigned char smem_raw[]; // sizeof(Shared) bytes
+  Shared &sh = *reinterpret_cast<Shared *>(smem_raw);
   __shared__ BoxDesc box_s;
   if (!items) {
     for (int item = blockIdx.x; item < nitems; item += gridDim.x) {

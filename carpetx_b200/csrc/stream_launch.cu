@@ -10,6 +10,10 @@ KernelFn kernel_part2(int pair);
 KernelFn kernel_part3(int pair);
 
 namespace {
+bool g_attr_set[kStreamPairs] = {};
+
+// Kernel of a pair; the first lookup allows its dynamic shared memory
+// (sizeof(Shared), which may exceed the 48 KB default).
 KernelFn kernel_for(int pair) {
   KernelFn k = kernel_part0(pair);
   if (!k)
@@ -18,6 +22,10 @@ KernelFn kernel_for(int pair) {
     k = kernel_part2(pair);
   if (!k)
     k = kernel_part3(pair);
+  if (k && pair >= 0 && pair < kStreamPairs && !g_attr_set[pair]) {
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Shared));
+    g_attr_set[pair] = true;
+  }
   return k;
 }
 
@@ -100,7 +108,7 @@ int stream_level_grid(int pair) {
     return 0;
   if (!g_grid[pair]) {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel_for(pair), NTS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel_for(pair), NTS, sizeof(Shared));
     g_grid[pair] = sms() * (per_sm > 0 ? per_sm : 1);
   }
   return g_grid[pair];
@@ -119,7 +127,7 @@ cudaError_t launch_stream_box(const BoxDesc &b, cudaStream_t s) {
     return cudaErrorInvalidValue;
   const int n = (int)n64;
   const int cap = stream_level_grid(pair);
-  k<<<n < cap ? n : cap, NTS, 0, s>>>(b, nullptr, nullptr, n);
+  k<<<n < cap ? n : cap, NTS, sizeof(Shared), s>>>(b, nullptr, nullptr, n);
   return cudaGetLastError();
 }
 
@@ -132,7 +140,7 @@ cudaError_t launch_stream_level(int pair, const BoxDesc *d_boxes, const TileRef 
   if (!k)
     return cudaErrorInvalidValue;
   BoxDesc unused{};
-  k<<<grid < nitems ? grid : nitems, NTS, 0, s>>>(unused, d_boxes, d_items, nitems);
+  k<<<grid < nitems ? grid : nitems, NTS, sizeof(Shared), s>>>(unused, d_boxes, d_items, nitems);
   return cudaGetLastError();
 }
 

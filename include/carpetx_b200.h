@@ -16,9 +16,13 @@
  * unless stated otherwise; work is enqueued on `stream` and returns without
  * synchronising, as the reference's GPU path does (impl.hxx:1685-1688).
  *
- * Results are bit-identical to the reference operators compiled for the host:
+ * Results equal the reference operators compiled for the host as FP64 values:
  * every stencil is evaluated with the reference's association order and
- * separately rounded products and sums (no FMA contraction). */
+ * separately rounded products and sums (no FMA contraction).  The separable
+ * operators skip the reference's initial "0 +" and its products by a
+ * coefficient of exactly 1, which are exact; the only bit pattern that can
+ * differ is the sign of a result that is exactly zero (-0 where the
+ * reference gives +0). */
 #ifndef CARPETX_B200_H
 #define CARPETX_B200_H
 
