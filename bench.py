@@ -23,6 +23,9 @@ One step = prolongation of every box and component of the level.  Reported:
   roofline   algorithmic bytes 8 (|CoarseBox(region)| + |region|) per box and
              component over the kernel time, against the measured HBM copy
              bandwidth
+  adjoint    forward and adjoint (P^T) time per pass of the differentiated
+             configuration (64 boxes, 32-96 coarse points per direction, 4
+             variables), one launch per box each, and their ratio
   cpu_baseline  the reference operators compiled for the host
              (oracle/_ref, all host threads, OpenMP over boxes) on one
              component of every box
@@ -62,6 +65,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--per-box-steps", type=int, default=2)
     p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--adjoint-steps", type=int, default=3,
+                   help="passes of the forward/adjoint comparison (0: skip)")
     p.add_argument("--boxes", type=int, default=512, help="level512: number of boxes")
     p.add_argument("--ncomp", type=int, default=24, help="level512: variables per box")
     return p.parse_args()
@@ -92,6 +97,61 @@ def workload(name, seed, nboxes=512, ncomp=24):
     return ([("conservative", 1, 7, (-3, -3, -3), (130, 130, 130), (0, 0, 0), (255, 255, 255), 8)],
             {"workload": "cons128: conservative o1 CCC, 128^3 -> 256^3 cells, 3 ghosts, 8 vars",
              "boxes": 1, "ncomp": 8})
+
+
+def adjoint_leg(args, cb, torch, dev, max_over_ranks, barrier):
+    """Forward and adjoint (P^T, cx_prolong_adjoint_box) of the differentiated
+    configuration, one launch per box each: 64 boxes with coarse points per
+    direction round(exp(U[ln 32, ln 96])), 4 components, alternately
+    interpolate order 5 VVV and conservative order 1 CCC, fine region = the
+    refined box.  Returns the per-pass times and their ratio."""
+    rng = np.random.default_rng(args.seed + 5)
+    boxes = []
+    for i in range(64):
+        n = np.round(np.exp(rng.uniform(np.log(32), np.log(96), 3))).astype(int)
+        typ, order, it = ("interpolate", 5, 0) if i % 2 == 0 else ("conservative", 1, 7)
+        cc = 1 if it == 7 else 0
+        flo = (0, 0, 0)
+        fhi = tuple(int(2 * n[d] - 1 - (1 - cc)) for d in range(3))
+        op = cb.Op(typ, order, it)
+        clo, chi = op.coarse_box(flo, fhi)
+        boxes.append((op, clo, chi, flo, fhi))
+    nc = 4
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(args.seed + 5)
+    data = []
+    for op, clo, chi, flo, fhi in boxes:
+        u = torch.randn((nc,) + box_shape(clo, chi), dtype=torch.float64, device=dev, generator=gen)
+        f = torch.empty((nc,) + box_shape(flo, fhi), dtype=torch.float64, device=dev)
+        ub = torch.empty_like(u)
+        data.append((op, u, clo, chi, f, flo, fhi, ub))
+    nfine = sum(nc * npts(b[5], b[6]) for b in data)
+
+    def fwd():
+        for op, u, clo, chi, f, flo, fhi, ub in data:
+            cb.prolong_box(op, u, clo, chi, f, flo, fhi, flo, fhi, nc)
+
+    def adj():
+        for op, u, clo, chi, f, flo, fhi, ub in data:
+            cb.prolong_adjoint_box(op, u, clo, chi, f, flo, fhi, flo, fhi, nc, ub)
+
+    out = {"workload": "64 boxes, coarse 32-96 points/dim log-uniform, 4 vars, interpolate o5 VVV "
+                       "/ conservative o1 CCC, one launch per box",
+           "fine_points": nfine}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for name, fn in (("fwd", fwd), ("adj", adj)):
+        for _ in range(2):
+            fn()
+        barrier()
+        e0.record()
+        for _ in range(args.adjoint_steps):
+            fn()
+        e1.record()
+        barrier()
+        out[name + "_ms"] = max_over_ranks(e0.elapsed_time(e1)) / args.adjoint_steps
+    out["adj_over_fwd"] = out["adj_ms"] / out["fwd_ms"]
+    del data
+    return out
 
 
 class ClockSampler:
@@ -390,6 +450,9 @@ def main():
         ms_e2e = max_over_ranks(e0.elapsed_time(e1)) / args.e2e_steps
         e2e_value = total_fine / (ms_e2e / 1e3)
 
+    adjoint = adjoint_leg(args, cb, torch, dev, max_over_ranks, barrier) if args.adjoint_steps > 0 \
+        else None
+
     peak, peak_src = measured_peaks()
     # per GPU: the ranks' mean algorithmic bytes over the slowest rank's time
     mean_bytes = sum_over_ranks(alg_bytes, dev) / world
@@ -421,6 +484,7 @@ def main():
                      "frac_of_8TBs_spec": achieved / 8000.0,
                      "step_ms_min": min(per_step), "step_ms_max": max(per_step)},
         "clocks": clk,
+        "adjoint": adjoint,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         lib, kind = cpu_lib()

@@ -199,3 +199,29 @@ def test_gpu_restrict_adjoint(dev, cx, it):
     want = np.zeros_like(f)
     cx.restrict_adjoint(it, g, clo, chi, want, flo, fhi, rlo, rhi, 2)
     np.testing.assert_array_equal(RTg.cpu().numpy(), want)
+
+
+@pytest.mark.parametrize("typ,order,it", [("interpolate", 5, 0), ("conservative", 1, 7),
+                                          ("hermite", 3, 3), ("interpolate", 7, 5),
+                                          ("conservative", 0, 2), ("natural", 7, 6)])
+def test_gpu_prolong_adjoint_tiled(dev, cx, typ, order, it):
+    """P^T on boxes that span several adjoint tiles in x and y and several z
+    chunks, with an odd region inside the fine box, against the oracle's
+    transpose; every coarse point is overwritten."""
+    rng = np.random.default_rng(100 + order * 8 + it)
+    flo, fhi = (-7, 3, -2), (196, 150, 29)
+    rlo, rhi = (-5, 4, -1), (193, 149, 28)
+    clo, chi = cx.coarse_box(typ, order, it, rlo, rhi)
+    clo = tuple(c - 1 for c in clo)  # one more coarse layer than the stencils read
+    op = cb.Op(typ, order, it)
+    u = rng.standard_normal((1,) + box_shape(clo, chi))
+    v = rng.standard_normal((1,) + box_shape(flo, fhi))
+    PTv = torch.full((1,) + box_shape(clo, chi), np.nan, dtype=torch.float64, device="cuda")
+    cb.prolong_adjoint_box(op, cuda(u), clo, chi, cuda(v), flo, fhi, rlo, rhi, 1, PTv)
+    torch.cuda.synchronize()
+    want = np.zeros_like(u)
+    cx.prolong_adjoint(typ, order, it, 0, u, clo, chi, v * region_mask(flo, fhi, rlo, rhi), flo,
+                       fhi, rlo, rhi, 1, want)
+    got = PTv.cpu().numpy()
+    assert not np.any(np.isnan(got)), "coarse points left unwritten"
+    np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12 * np.max(np.abs(want)))
