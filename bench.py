@@ -25,7 +25,8 @@ One step = prolongation of every box and component of the level.  Reported:
              bandwidth
   adjoint    forward and adjoint (P^T) time per pass of the differentiated
              configuration (64 boxes, 32-96 coarse points per direction, 4
-             variables), one launch per box each, and their ratio
+             variables), as level plans and one launch per box, and the
+             adjoint/forward ratios
   cpu_baseline  the reference operators compiled for the host
              (oracle/_ref, all host threads, OpenMP over boxes) on one
              component of every box
@@ -135,11 +136,20 @@ def adjoint_leg(args, cb, torch, dev, max_over_ranks, barrier):
         for op, u, clo, chi, f, flo, fhi, ub in data:
             cb.prolong_adjoint_box(op, u, clo, chi, f, flo, fhi, flo, fhi, nc, ub)
 
+    def plan_boxes(out_crse):
+        return [dict(op=op, ncomp=nc, crse=ub if out_crse else u, crse_lo=clo, crse_hi=chi,
+                     fine=f, fine_lo=flo, fine_hi=fhi, reg_lo=flo, reg_hi=fhi)
+                for op, u, clo, chi, f, flo, fhi, ub in data]
+
+    plan_f = cb.LevelPlan(plan_boxes(False))
+    plan_a = cb.LevelPlan(plan_boxes(True), adjoint=True)
     out = {"workload": "64 boxes, coarse 32-96 points/dim log-uniform, 4 vars, interpolate o5 VVV "
-                       "/ conservative o1 CCC, one launch per box",
+                       "/ conservative o1 CCC; level plans (one persistent launch per stencil "
+                       "pair) and one launch per box",
            "fine_points": nfine}
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for name, fn in (("fwd", fwd), ("adj", adj)):
+    for name, fn in (("fwd_level", plan_f.execute), ("adj_level", plan_a.execute),
+                     ("fwd_per_box", fwd), ("adj_per_box", adj)):
         for _ in range(2):
             fn()
         barrier()
@@ -149,7 +159,11 @@ def adjoint_leg(args, cb, torch, dev, max_over_ranks, barrier):
         e1.record()
         barrier()
         out[name + "_ms"] = max_over_ranks(e0.elapsed_time(e1)) / args.adjoint_steps
-    out["adj_over_fwd"] = out["adj_ms"] / out["fwd_ms"]
+    out["adj_over_fwd"] = out["adj_level_ms"] / out["fwd_level_ms"]
+    out["adj_over_fwd_per_box"] = out["adj_per_box_ms"] / out["fwd_per_box_ms"]
+    out["adj_level_gbs"] = plan_a.stats()["bytes"] / (out["adj_level_ms"] / 1e3) / 1e9
+    plan_f.close()
+    plan_a.close()
     del data
     return out
 

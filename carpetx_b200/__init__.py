@@ -72,6 +72,8 @@ def lib():
         L.cx_prolong_box_diag.argtypes = [ctypes.c_int32, _VP, _I3, _I3, _VP, _I3, _I3, _I3, _I3,
                                           _I, _I, _VP, _VP, _VP]
         L.cx_level_plan_create.argtypes = [ctypes.POINTER(CxBox), _I, _I, ctypes.POINTER(_VP)]
+        L.cx_level_plan_create_adjoint.argtypes = [ctypes.POINTER(CxBox), _I, _I,
+                                                   ctypes.POINTER(_VP)]
         L.cx_level_plan_execute.argtypes = [_VP, _VP]
         L.cx_level_plan_stats.argtypes = [_VP, ctypes.POINTER(ctypes.c_int64),
                                           ctypes.POINTER(ctypes.c_int64),
@@ -195,9 +197,11 @@ class LevelPlan:
 
     boxes: iterable of dicts with keys op, ncomp, crse, crse_lo, crse_hi, fine,
     fine_lo, fine_hi, reg_lo, reg_hi (tensors as for prolong_box).  The plan
-    keeps references to the tensors so their memory outlives it."""
+    keeps references to the tensors so their memory outlives it.  With
+    adjoint=True (cx_level_plan_create_adjoint) executing the plan overwrites
+    every crse tensor with P^T of its fine tensor (region points only)."""
 
-    def __init__(self, boxes, per_group=False):
+    def __init__(self, boxes, per_group=False, adjoint=False):
         self._keep = []
         arr = (CxBox * max(1, len(boxes)))()
         for i, b in enumerate(boxes):
@@ -210,7 +214,8 @@ class LevelPlan:
                            _i3(b["reg_hi"]))
             self._keep += [b["crse"], b["fine"]]
         h = ctypes.c_void_p()
-        _check(lib().cx_level_plan_create(arr, len(boxes), int(bool(per_group)), ctypes.byref(h)))
+        create = lib().cx_level_plan_create_adjoint if adjoint else lib().cx_level_plan_create
+        _check(create(arr, len(boxes), int(bool(per_group)), ctypes.byref(h)))
         self.handle = h
 
     def execute(self, stream=None):

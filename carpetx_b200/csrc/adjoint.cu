@@ -1,5 +1,5 @@
 // Transpose of the separable linear prolongations, streaming gather form (no
-// atomics).
+// atomics), for one box per launch or a whole level per persistent launch.
 //
 // P = Pz Py Px (the x pass first) with 1-D maps P_d, so P^T = Px^T Py^T Pz^T
 // and the three 1-D transposes can be applied in any order.  In 1-D, fine
@@ -12,9 +12,13 @@
 // A work item is a tile of up to NU coarse (x, y) columns of the coarse box
 // over a chunk of coarse z, one component.  The CTA streams the fine z planes
 // that reach the chunk through a ring of shared-memory buffers holding the
-// tile's fine footprint (the region's fine points of it; the rest of the
-// footprint is zero, set once per item):
-//   load   fine plane fz + DPF (asynchronous 8-byte copies, one warp per row);
+// tile's fine footprint (its region points; the rest of the footprint reads
+// as zero):
+//   load   fine plane fz + DPF: one thread per footprint row issues one bulk
+//          (TMA) copy of the row's 16-byte aligned middle, completing on the
+//          buffer's mbarrier (each row is placed in shared memory with the
+//          parity of its global address, so both ends of the copy are 16-byte
+//          aligned); the odd first/last point of a row takes an 8-byte copy;
 //   x^T    G(cx, fy) for the tile's coarse x and every footprint row, XB
 //          coarse x per task from a register window of the fine row, into
 //          shared memory (column major: the y taps of a column are adjacent);
@@ -25,8 +29,8 @@
 //          cc + RLO is complete and is stored.
 // Every coarse point of the coarse box is written once (zero where no region
 // point reads it); sums run in a fixed order, so results are deterministic.
-// Fine data is read once per item plus the tile's footprint halo (served by
-// the L2 when neighbouring tiles stream together).
+// Fine data is read from HBM once; the footprint halo of a tile is read again
+// by its neighbours, from the L2 (tiles of a box are dealt together).
 #include <type_traits>
 
 #include "cx_internal.h"
@@ -98,35 +102,53 @@ template <class K> CXB_HD constexpr double wtap(int m) {
 }
 template <class K> constexpr int DK = K::RHI - K::RLO;
 
-constexpr int NT = 256;        // threads per CTA
-constexpr int UPT = 2;         // coarse columns per thread
-constexpr int NU = NT * UPT;   // coarse columns per item at most
-constexpr int TMAX = 64;       // tile extent in x or y at most
-constexpr int DPF = 2;         // fine planes prefetched ahead
-constexpr int NBUF = DPF + 1;  // shared fine-plane ring
-constexpr int XB = 4;          // coarse x per x^T task
+// One CTA of NT threads per SM streams a tile of up to NT x UPT coarse
+// columns (at most TMAX per direction): large tiles keep the footprint halo,
+// loaded and transposed in x once more per tile, small (a 39 x 39 tile of
+// the order-5 stencils reads 1.27 fine points per point it owns).  A plane of
+// such a tile is several microseconds of work, so one plane prefetched ahead
+// covers the DRAM latency.
+constexpr int NT = 512;       // threads per CTA
+constexpr int TMAX = 64;      // tile extent in x or y at most
+constexpr int DPF = 1;        // fine planes prefetched ahead
+constexpr int NBUF = DPF + 1; // shared fine-plane ring
+constexpr int XB = 4;         // coarse x per x^T task
 
-// Footprint of a TX x TY tile for stencil spread D (<= DM): rows, row pitch
-// (odd), and x^T column pitch (odd).
+// Footprint of a TX x TY tile for stencil spread D <= DM: rows, row pitch
+// (odd, one more than the widest footprint row: a row is placed at offset 0
+// or 1 to match its global address parity), x^T column pitch (odd).
 CXB_HD constexpr int fp_rows(int ty, int dm) { return 2 * ty + 2 * dm; }
-CXB_HD constexpr int fp_pitch(int tx, int dm) { return (2 * tx + 2 * dm) | 1; }
+CXB_HD constexpr int fp_pitch(int tx, int dm) { return 2 * tx + 2 * dm + 1; }
 CXB_HD constexpr int g_pitch(int ty, int dm) { return fp_rows(ty, dm) | 1; }
-CXB_HD constexpr int tile_ty(int tx) { return NU / tx < TMAX ? NU / tx : TMAX; }
-CXB_HD constexpr int max_fp(int dm, int what) {
+CXB_HD constexpr int tile_ty(int tx, int nu) { return nu / tx < TMAX ? nu / tx : TMAX; }
+CXB_HD constexpr int max_fp(int dm, int nu, int what) {
   int m = 0;
   for (int tx = 1; tx <= TMAX; ++tx) {
-    const int ty = tile_ty(tx);
-    const int v = what == 0 ? fp_rows(ty, dm) * fp_pitch(tx, dm) : tx * g_pitch(ty, dm);
+    const int ty = tile_ty(tx, nu);
+    const int nseg = (tx + XB - 1) / XB;
+    const int v = what == 0   ? fp_rows(ty, dm) * fp_pitch(tx, dm)
+                  : what == 1 ? tx * g_pitch(ty, dm)
+                              : nseg * fp_rows(ty, dm);
     m = v > m ? v : m;
   }
   return m;
 }
+// coarse columns per thread, as many as the registers hold next to the
+// ring of RHI - RLO + 1 partial sums per column: 4 up to spread 4, 3 for the
+// order-5 stencils, 2 for order 7
+CXB_HD constexpr int upt_of(int dm) { return dm <= 4 ? 4 : dm <= 6 ? 3 : 2; }
 
 template <class KV, class KC> struct AdjPair {
   static constexpr int DM = DK<KV> > DK<KC> ? DK<KV> : DK<KC>;
-  static constexpr int FP = max_fp(DM, 0); // fine footprint plane (doubles)
-  static constexpr int GP = max_fp(DM, 1); // x^T result (doubles)
+  static constexpr int UPT = upt_of(DM);
+  static constexpr int NU = NT * UPT; // coarse columns per item at most
+  static constexpr int FP = (max_fp(DM, NU, 0) + 1) & ~1; // fine footprint plane (even: 16-byte buffers)
+  static constexpr int GP = max_fp(DM, NU, 1);            // x^T result
+  static constexpr int XTMAX = (max_fp(DM, NU, 2) + NT - 1) / NT; // x^T tasks per thread
+  // the last x^T window of a row may run 2 (XB - 1) points past the row
   static constexpr size_t SMEM = sizeof(double) * (size_t)(NBUF * FP + GP + 2 * XB);
+  static_assert(SMEM + 1024 <= 227 * 1024, "shared memory per CTA");
+  static_assert(XTMAX <= 3, "x^T task registers");
 };
 
 __device__ __forceinline__ void cp_async8(double *sdst, const double *gsrc) {
@@ -139,29 +161,63 @@ __device__ __forceinline__ void cp_async_wait_dpf() {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-struct AdjTiling {
-  int tx, ty, tz;    // coarse tile extents (x, y) and coarse z per item
-  int ntx, nty, ntz; // tiles per direction
-};
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *m, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(m)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *m, uint32_t bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(m)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *m) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(
+                   smem_u32(m))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *m, uint32_t parity) {
+  uint32_t ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+               " selp.u32 %0, 1, 0, p;\n}\n"
+               : "=r"(ok)
+               : "r"(smem_u32(m)), "r"(parity)
+               : "memory");
+  return ok != 0;
+}
+// Waits for the phase of parity `parity` to complete, for about a second at
+// most (clock cycles); false if it gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *m, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_try(m, parity))
+    if (clock64() - t0 > (1ll << 31))
+      return false;
+  return true;
+}
+// Bulk copy global -> this CTA's shared memory (no multicast), completing
+// `bytes` on mbarrier m; both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *m) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+               "[%3];\n" ::"r"(smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(m))
+               : "memory");
+}
+// Orders this thread's generic-proxy shared-memory accesses before later
+// async-proxy (bulk copy) accesses.
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
 
-// Per-item geometry.
-struct AItem {
-  int cx0, cy0, cz0, cz1; // tile origin (coarse, absolute), coarse z chunk
-  int txe, tye;           // tile extent
-  int fxo, fyo;           // footprint origin (fine, absolute)
-  int fw, fh, fpw, gpw;   // footprint width, rows, row pitch; x^T column pitch
-  int ax, bx, ay, by;     // region part of the footprint (local, inclusive)
-  int fa, fb;             // fine planes streamed
-  const double *fbase;    // fine component base at (flo)
-  int fnx;
-  int64_t fplane;
-  int flo_z;
-};
+// Set when a bounded wait gave up (read and cleared by cx_check_device).
+__device__ int g_adj_timeout = 0;
 
 // x^T task: XB coarse x of one footprint row from a register window; only
-// the first n are stored (the window of the last task of a row may run up to
-// 2 (XB - 1) points past the footprint: those reach only unstored results,
-// and the shared allocation is padded for them).
+// the first n are stored (the window of the last task of a row may run past
+// the row: those points reach only unstored results).
 template <class K>
 __device__ __forceinline__ void xt_task(const double *__restrict__ src, double *__restrict__ dst,
                                         int gpw, int n) {
@@ -197,57 +253,135 @@ template <class K> __device__ __forceinline__ double yt_col(const double *__rest
   return acc;
 }
 
+// z^T: fine plane with offset OFF adds w(OFF, RLO + k) g to partial sum k.
+template <class K, int OFF, int L>
+__device__ __forceinline__ void zt_add(double (&acc)[L], double g) {
+#pragma unroll
+  for (int k = 0; k < L; ++k) {
+    const double w = Weight<K>::w(OFF, K::RLO + k);
+    if (w != 0.0)
+      acc[k] = fma(w, g, acc[k]);
+  }
+}
+
+// One item: coarse tile (xt, yt), coarse z chunk zt, component comp of box b.
+// Returns false if a bounded wait gave up (the CTA then stops).
 template <class KV, class KC, class KZ>
-__device__ __forceinline__ void adj_item(double *fbuf, double *gbuf, const BoxDesc &b,
-                                         const AItem &it, double *__restrict__ out) {
-  constexpr int FP = AdjPair<KV, KC>::FP;
+__device__ __forceinline__ bool adj_item(double *fbuf, double *gbuf, uint64_t *mbar, int *s_fail,
+                                         uint32_t &phase, const BoxDesc &bd, int xt, int yt, int zt,
+                                         int comp) {
+  constexpr int FP = AdjPair<KV, KC>::FP, DM = AdjPair<KV, KC>::DM;
+  constexpr int UPT = AdjPair<KV, KC>::UPT, XTMAX = AdjPair<KV, KC>::XTMAX;
   constexpr int L = DK<KZ> + 1;
-  const int ccx = kind_info(b.kind[0]).cent, ccy = kind_info(b.kind[1]).cent;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tid = threadIdx.x;
+  // the descriptor fields used below, in registers
+  const int kx = bd.kind[0], ky = bd.kind[1];
+  const bool ccx = kind_info(kx).cent == CC, ccy = kind_info(ky).cent == CC;
+  const int cnx = bd.cnx, cny = bd.cny, fnx = bd.fnx;
+  const int64_t cplane = (int64_t)cnx * cny, fplane = (int64_t)fnx * bd.fny;
+  const int cnz = (int)(bd.cnp / cplane);
+  const int clo0 = bd.clo[0], clo1 = bd.clo[1], clo2 = bd.clo[2];
+  const int cx0 = clo0 + xt * bd.at[0], cy0 = clo1 + yt * bd.at[1], cz0 = clo2 + zt * bd.at[2];
+  const int txe = min(bd.at[0], clo0 + cnx - cx0), tye = min(bd.at[1], clo1 + cny - cy0);
+  const int cz1 = min(cz0 + bd.at[2] - 1, clo2 + cnz - 1);
+  const int rhx = sep_rhi(kx), dx = rhx - sep_rlo(kx);
+  const int rhy = sep_rhi(ky), dy = rhy - sep_rlo(ky);
+  const int fxo = 2 * (cx0 - rhx), fyo = 2 * (cy0 - rhy);
+  const int fw = 2 * txe + 2 * dx, fh = 2 * tye + 2 * dy;
+  const int fpw = fp_pitch(txe, DM), gpw = g_pitch(tye, DM);
+  const int ax = max(0, bd.rlo[0] - fxo), bx = min(fw - 1, bd.rhi[0] - fxo);
+  const int ay = max(0, bd.rlo[1] - fyo), by = min(fh - 1, bd.rhi[1] - fyo);
+  int fa = max(2 * (cz0 - KZ::RHI), bd.rlo[2]);
+  int fb = min(2 * (cz1 - KZ::RLO) + 1, bd.rhi[2]);
+  if (ax > bx || ay > by) { // no region point in the footprint
+    fa = 1;
+    fb = 0;
+  }
+  const double *fcomp = bd.fine + comp * bd.fnp; // fine_bar component
+  const uint64_t fcomp8 = (uint64_t)(uintptr_t)fcomp >> 3;
+  // element offset of footprint point (0, 0) of fine plane fz in the component
+  const int64_t org = (int64_t)(fyo - bd.flo[1]) * fnx + (fxo - bd.flo[0]) - (int64_t)bd.flo[2] * fplane;
+  const int dpar = (fnx + fpw) & 1; // row r sits at r fpw + ((parity of plane) + r dpar) % 2
+  const bool edge = ax > 0 || bx < fw - 1; // region rows have columns outside the region
+  double *out = bd.cbar + comp * bd.cnp;
 
-  // zero the footprint of every buffer once: points outside the region stay 0
-  for (int k = 0; k < NBUF; ++k)
-    for (int e = tid; e < it.fh * it.fpw; e += NT)
-      fbuf[k * FP + e] = 0.0;
-  __syncthreads();
-
-  auto load = [&](int fz, int k) {
-    const double *pl = it.fbase + (int64_t)(fz - it.flo_z) * it.fplane;
-    double *S = fbuf + k * FP;
-    for (int r = it.ay + warp; r <= it.by; r += NT / 32) {
-      const double *row = pl + (int64_t)(it.fyo + r - b.flo[1]) * it.fnx + (it.fxo - b.flo[0]);
-      for (int c = it.ax + lane; c <= it.bx; c += 32)
-        cp_async8(S + r * it.fpw + c, row + c);
-    }
-  };
-
-  // this thread's columns
-  int ui[UPT], uj[UPT];
-  bool act[UPT];
+  // this thread's columns: y^T source in the x^T result, output offset
+  int ysrc[UPT], cofs[UPT];
 #pragma unroll
   for (int q = 0; q < UPT; ++q) {
     const int u = tid + q * NT;
-    uj[q] = u / it.txe;
-    ui[q] = u - uj[q] * it.txe;
-    act[q] = uj[q] < it.tye;
+    const int uj = u / txe, ui = u - uj * txe;
+    ysrc[q] = uj < tye ? ui * gpw + 2 * uj : -1;
+    cofs[q] = (cy0 + uj - clo1) * cnx + (cx0 + ui - clo0);
   }
+  // this thread's x^T tasks: (segment s, row r), rows fastest
+  int xsrc[XTMAX], xdst[XTMAX], xodd[XTMAX], xn[XTMAX];
+  const int nseg = (txe + XB - 1) / XB;
+#pragma unroll
+  for (int k = 0; k < XTMAX; ++k) {
+    const int t = tid + k * NT;
+    const int s = t / fh, r = t - s * fh;
+    xn[k] = s < nseg ? min(XB, txe - s * XB) : 0;
+    xsrc[k] = r * fpw + 2 * XB * s;
+    xdst[k] = s * XB * gpw + r;
+    xodd[k] = r & dpar;
+  }
+
+  // zero every buffer's footprint once: rows outside the region stay zero;
+  // the columns of region rows outside the region are zeroed with each load
+  for (int k = 0; k < NBUF; ++k)
+    for (int e = tid; e < fh * fpw; e += NT)
+      fbuf[k * FP + e] = 0.0;
+  fence_proxy_async();
+  __syncthreads();
+
+  // issue the copies of fine plane fz into buffer k (the buffer's mbarrier
+  // receives the bulk bytes; thread 0 arrives once every thread has issued)
+  auto load = [&](int fz, int k) {
+    double *S = fbuf + k * FP;
+    const int r = ay + tid; // footprint rows <= NT
+    if (r <= by) {
+      const int64_t rofs = org + (int64_t)fz * fplane + (int64_t)r * fnx; // (r, 0)
+      const int par = (int)((fcomp8 + (uint64_t)rofs) & 1);
+      const int rb = r * fpw + ((par + r * fpw) & 1); // same parity as the row's address
+      const double *rowg = fcomp + rofs;
+      const int c0 = ax + ((par + ax) & 1); // first column with a 16-byte aligned address
+      const int nch = (bx - c0 + 1) >> 1;
+      if (nch > 0) {
+        mbar_expect_tx(mbar + k, 16u * (uint32_t)nch);
+        bulk_g2s(S + rb + c0, rowg + c0, 16u * (uint32_t)nch, mbar + k);
+      }
+      if (c0 > ax)
+        cp_async8(S + rb + ax, rowg + ax);
+      const int cl = c0 + 2 * nch;
+      if (cl <= bx)
+        cp_async8(S + rb + cl, rowg + cl);
+      if (edge) {
+        for (int c = 0; c < ax; ++c)
+          S[rb + c] = 0.0;
+        for (int c = bx + 1; c < fw; ++c)
+          S[rb + c] = 0.0;
+        fence_proxy_async();
+      }
+    }
+  };
+
   double acc[UPT][L];
 #pragma unroll
   for (int q = 0; q < UPT; ++q)
 #pragma unroll
     for (int k = 0; k < L; ++k)
       acc[q][k] = 0.0;
-  const int64_t cplane = (int64_t)b.cnx * b.cny;
-  int cc = it.cz0 - KZ::RHI; // acc[q][k] <-> coarse plane cc + RLO + k
+  int cc = cz0 - KZ::RHI; // acc[q][k] <-> coarse plane cc + RLO + k
   auto advance_to = [&](int target) {
     for (; cc < target; ++cc) {
       const int cz = cc + KZ::RLO;
-      if (cz >= it.cz0 && cz <= it.cz1) {
+      if (cz >= cz0 && cz <= cz1) {
+        double *o = out + (int64_t)(cz - clo2) * cplane;
 #pragma unroll
         for (int q = 0; q < UPT; ++q)
-          if (act[q])
-            out[(int64_t)(cz - b.clo[2]) * cplane + (int64_t)(it.cy0 + uj[q] - b.clo[1]) * b.cnx +
-                (it.cx0 + ui[q] - b.clo[0])] = acc[q][0];
+          if (ysrc[q] >= 0)
+            o[cofs[q]] = acc[q][0];
       }
 #pragma unroll
       for (int q = 0; q < UPT; ++q) {
@@ -259,121 +393,137 @@ __device__ __forceinline__ void adj_item(double *fbuf, double *gbuf, const BoxDe
     }
   };
 
-  const int nseg = (it.txe + XB - 1) / XB;
-  const int ntask = nseg * it.fh;
 #pragma unroll
   for (int d = 0; d < DPF; ++d) {
-    if (it.fa + d <= it.fb)
-      load(it.fa + d, d);
+    if (fa + d <= fb)
+      load(fa + d, d);
     cp_async_commit();
   }
+  __syncthreads();
+  if (tid == 0)
+    for (int d = 0; d < DPF; ++d)
+      if (fa + d <= fb)
+        mbar_arrive(mbar + d);
   int slot = 0;
-  for (int fz = it.fa; fz <= it.fb; ++fz) {
-    {
-      int ls = slot + DPF;
-      if (ls >= NBUF)
-        ls -= NBUF;
-      if (fz + DPF <= it.fb)
-        load(fz + DPF, ls);
-      cp_async_commit();
-    }
+  for (int fz = fa; fz <= fb; ++fz) {
+    int ls = slot + DPF;
+    if (ls >= NBUF)
+      ls -= NBUF;
+    const bool more = fz + DPF <= fb;
+    if (more)
+      load(fz + DPF, ls);
+    cp_async_commit();
     cp_async_wait_dpf();
+    const uint32_t par = (phase >> slot) & 1u;
+    if (tid == 0 && !mbar_wait_bounded(mbar + slot, par)) {
+      *s_fail = 1;
+      g_adj_timeout = 1;
+    }
     __syncthreads();
+    if (*s_fail) {
+      // stop: let the copies issued for the next plane land first (bounded)
+      if (tid == 0 && more) {
+        mbar_arrive(mbar + ls);
+        mbar_wait_bounded(mbar + ls, (phase >> ls) & 1u);
+      }
+      cp_async_wait_all();
+      __syncthreads();
+      return false;
+    }
+    if (tid == 0 && more)
+      mbar_arrive(mbar + ls); // every thread issued its copies before the barrier
+    mbar_try(mbar + slot, par); // completed: acquires the bulk data for this thread
+    phase ^= 1u << slot;
     const double *S = fbuf + slot * FP;
-    for (int k = tid; k < ntask; k += NT) {
-      const int s = k / it.fh, r = k - s * it.fh;
-      const int n = min(XB, it.txe - s * XB);
-      const double *src = S + r * it.fpw + 2 * XB * s;
-      double *dst = gbuf + (s * XB) * it.gpw + r;
+    const int p0 = (int)((fcomp8 + (uint64_t)(org + (int64_t)fz * fplane)) & 1);
+#pragma unroll
+    for (int k = 0; k < XTMAX; ++k) {
+      if (xn[k] <= 0)
+        continue;
+      const double *src = S + xsrc[k] + ((p0 + xodd[k]) & 1);
       if (ccx)
-        xt_task<KC>(src, dst, it.gpw, n);
+        xt_task<KC>(src, gbuf + xdst[k], gpw, xn[k]);
       else
-        xt_task<KV>(src, dst, it.gpw, n);
+        xt_task<KV>(src, gbuf + xdst[k], gpw, xn[k]);
     }
     __syncthreads();
     advance_to(fz >> 1);
-    const int off = fz & 1;
 #pragma unroll
     for (int q = 0; q < UPT; ++q) {
-      if (!act[q])
+      if (ysrc[q] < 0)
         continue;
-      const double *src = gbuf + ui[q] * it.gpw + 2 * uj[q];
-      const double g = ccy ? yt_col<KC>(src) : yt_col<KV>(src);
-#pragma unroll
-      for (int k = 0; k < L; ++k) {
-        const double w0 = Weight<KZ>::w(0, KZ::RLO + k), w1 = Weight<KZ>::w(1, KZ::RLO + k);
-        const double w = off ? w1 : w0;
-        if (w0 != 0.0 || w1 != 0.0)
-          acc[q][k] = fma(w, g, acc[q][k]);
-      }
+      const double g = ccy ? yt_col<KC>(gbuf + ysrc[q]) : yt_col<KV>(gbuf + ysrc[q]);
+      if (fz & 1)
+        zt_add<KZ, 1, L>(acc[q], g);
+      else
+        zt_add<KZ, 0, L>(acc[q], g);
     }
     if (++slot == NBUF)
       slot = 0;
   }
-  advance_to(it.cz1 - KZ::RLO + 1);
+  advance_to(cz1 - KZ::RLO + 1);
   cp_async_wait_all();
   __syncthreads(); // the next item reuses the shared buffers
+  return true;
 }
 
+constexpr int BOX_WORDS = (int)(sizeof(BoxDesc) / sizeof(int));
+static_assert(BOX_WORDS <= NT, "one thread per descriptor word");
+
+// Box mode (items == nullptr): the items of box b strided over the grid.
+// Level mode: items of a device work list (sorted by cost, the tiles of a box
+// together) strided over persistent CTAs.
 template <class KV, class KC>
-__global__ void __launch_bounds__(NT, AdjPair<KV, KC>::SMEM > 110 * 1024 ? 1 : 2)
-    adjoint_kernel(const BoxDesc b, const AdjTiling t, double *crse_bar) {
+__global__ void __launch_bounds__(NT, 1)
+    adjoint_kernel(const __grid_constant__ BoxDesc b, const BoxDesc *__restrict__ boxes,
+                   const TileRef *__restrict__ items, int nitems) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ BoxDesc box_s;
+  __shared__ uint64_t mbar[NBUF];
+  __shared__ int s_fail;
   double *fbuf = reinterpret_cast<double *>(smem_raw);
   double *gbuf = fbuf + NBUF * AdjPair<KV, KC>::FP;
-  constexpr int DM = AdjPair<KV, KC>::DM;
-  const int nitems = t.ntx * t.nty * t.ntz * b.ncomp;
-  const int kx = b.kind[0], ky = b.kind[1];
-  const bool ccz = kind_info(b.kind[2]).cent == CC;
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < NBUF; ++k)
+      mbar_init(mbar + k, 1);
+    mbar_fence_init();
+    s_fail = 0;
+  }
+  __syncthreads();
+  uint32_t phase = 0; // completed-phase parity per buffer
   for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-    int r = item;
-    const int xt = r % t.ntx;
-    r /= t.ntx;
-    const int yt = r % t.nty;
-    r /= t.nty;
-    const int zt = r % t.ntz;
-    const int comp = r / t.ntz;
-    AItem it;
-    it.cx0 = b.clo[0] + xt * t.tx;
-    it.cy0 = b.clo[1] + yt * t.ty;
-    it.cz0 = b.clo[2] + zt * t.tz;
-    const int chi0 = b.clo[0] + b.cnx - 1, chi1 = b.clo[1] + b.cny - 1;
-    const int chi2 = b.clo[2] + (int)(b.cnp / ((int64_t)b.cnx * b.cny)) - 1;
-    it.txe = min(t.tx, chi0 - it.cx0 + 1);
-    it.tye = min(t.ty, chi1 - it.cy0 + 1);
-    it.cz1 = min(it.cz0 + t.tz - 1, chi2);
-    const int rhx = sep_rhi(kx), rhy = sep_rhi(ky);
-    const int dx = rhx - sep_rlo(kx), dy = rhy - sep_rlo(ky);
-    it.fxo = 2 * (it.cx0 - rhx);
-    it.fyo = 2 * (it.cy0 - rhy);
-    it.fw = 2 * it.txe + 2 * dx;
-    it.fh = 2 * it.tye + 2 * dy;
-    it.fpw = fp_pitch(it.txe, DM);
-    it.gpw = g_pitch(it.tye, DM);
-    it.ax = max(0, b.rlo[0] - it.fxo);
-    it.bx = min(it.fw - 1, b.rhi[0] - it.fxo);
-    it.ay = max(0, b.rlo[1] - it.fyo);
-    it.by = min(it.fh - 1, b.rhi[1] - it.fyo);
-    const int rlz = ccz ? KC::RLO : KV::RLO, rhz = ccz ? KC::RHI : KV::RHI;
-    it.fa = max(2 * (it.cz0 - rhz), b.rlo[2]);
-    it.fb = min(2 * (it.cz1 - rlz) + 1, b.rhi[2]);
-    if (it.ax > it.bx || it.ay > it.by) { // no region point in the footprint
-      it.fa = 1;
-      it.fb = 0;
+    const BoxDesc *bp = &b;
+    int xt, yt, zt, comp;
+    if (items) {
+      const TileRef t = items[item];
+      if (threadIdx.x < BOX_WORDS)
+        reinterpret_cast<int *>(&box_s)[threadIdx.x] =
+            reinterpret_cast<const int *>(boxes + t.box)[threadIdx.x];
+      __syncthreads();
+      bp = &box_s;
+      xt = t.tx;
+      yt = t.ty;
+      zt = t.tz;
+      comp = t.comp;
+    } else {
+      int r = item;
+      xt = r % b.ant[0];
+      r /= b.ant[0];
+      yt = r % b.ant[1];
+      r /= b.ant[1];
+      zt = r % b.ant[2];
+      comp = r / b.ant[2];
     }
-    it.fbase = b.fine + comp * b.fnp;
-    it.fnx = b.fnx;
-    it.fplane = (int64_t)b.fnx * b.fny;
-    it.flo_z = b.flo[2];
-    double *out = crse_bar + comp * b.cnp;
-    if (ccz)
-      adj_item<KV, KC, KC>(fbuf, gbuf, b, it, out);
-    else
-      adj_item<KV, KC, KV>(fbuf, gbuf, b, it, out);
+    const bool ok = kind_info(bp->kind[2]).cent == CC
+                        ? adj_item<KV, KC, KC>(fbuf, gbuf, mbar, &s_fail, phase, *bp, xt, yt, zt, comp)
+                        : adj_item<KV, KC, KV>(fbuf, gbuf, mbar, &s_fail, phase, *bp, xt, yt, zt, comp);
+    if (!ok)
+      return;
+    // adj_item ends with a barrier: box_s may be overwritten
   }
 }
 
-using AdjFn = void (*)(const BoxDesc, const AdjTiling, double *);
+using AdjFn = void (*)(const BoxDesc, const BoxDesc *, const TileRef *, int);
 
 // Kernel and shared-memory size of a pair (nullptr for the nonlinear ones).
 template <class V, class C> AdjFn adj_fn(size_t *smem) {
@@ -398,58 +548,121 @@ AdjFn adj_kernel(int pair, size_t *smem) {
   return nullptr;
 }
 
+template <class V, class C> int adj_upt_of() {
+  if constexpr (std::is_same_v<C, CcMinmod>)
+    return 0;
+  else
+    return AdjPair<V, C>::UPT;
+}
+
+// Coarse columns per thread of a pair's kernel.
+int adj_upt(int pair) {
+  switch (pair) {
+#define CXB_ADJ_UPT(I, V, C, KVI, KCI)                                         \
+  case I:                                                                      \
+    return adj_upt_of<V, C>();
+    CXB_STREAM_PAIRS(CXB_ADJ_UPT)
+#undef CXB_ADJ_UPT
+  default:
+    break;
+  }
+  return 2;
+}
+
 bool g_adj_attr[kStreamPairs] = {};
 int g_adj_grid[kStreamPairs] = {};
 
-AdjTiling adj_tiling(const BoxDesc &b, int min_items) {
-  AdjTiling t;
-  const int cnz = (int)(b.cnp / ((int64_t)b.cnx * b.cny));
-  t.ntx = (b.cnx + TMAX - 1) / TMAX;
-  t.tx = (b.cnx + t.ntx - 1) / t.ntx;
-  const int tymax = tile_ty(t.tx);
-  t.nty = (b.cny + tymax - 1) / tymax;
-  t.ty = (b.cny + t.nty - 1) / t.nty;
-  // coarse z per item: up to 48 (the z footprint costs 2 (RHI - RLO) fine
-  // planes per item), shorter (down to 8) until the box fills min_items CTAs
-  int maxz = 48;
-  const int64_t xy = (int64_t)t.ntx * t.nty * b.ncomp;
-  while (maxz > 8 && xy * ((cnz + maxz - 1) / maxz) < min_items)
-    maxz /= 2;
-  t.ntz = (cnz + maxz - 1) / maxz;
-  t.tz = (cnz + t.ntz - 1) / t.ntz;
-  t.ntz = (cnz + t.tz - 1) / t.tz;
-  return t;
+// Kernel of a pair, its dynamic shared memory allowed and its persistent
+// grid (SMs x resident CTAs) recorded on first use.
+AdjFn adj_ready(int pair, size_t *smem) {
+  AdjFn k = pair >= 0 && pair < kStreamPairs ? adj_kernel(pair, smem) : nullptr;
+  if (k && !g_adj_attr[pair]) {
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem) !=
+        cudaSuccess)
+      return nullptr;
+    int per_sm = 0, dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, *smem);
+    g_adj_grid[pair] = sms * (per_sm > 0 ? per_sm : 1);
+    g_adj_attr[pair] = true;
+  }
+  return k;
 }
 
 } // namespace
 
-cudaError_t launch_prolong_adjoint_box(const BoxDesc &b, int per_group, double *crse_bar,
+int adjoint_take_timeout() {
+  int v = 0, zero = 0;
+  if (cudaMemcpyFromSymbol(&v, g_adj_timeout, sizeof v) != cudaSuccess)
+    return -1;
+  if (v)
+    cudaMemcpyToSymbol(g_adj_timeout, &zero, sizeof zero);
+  return v;
+}
+
+int adjoint_pair_of(const BoxDesc &b) {
+  for (int d = 0; d < 3; ++d)
+    if (b.kind[d] == K_CC_MINMOD1 || b.kind[d] == K_CC_ENO2)
+      return -1;
+  return stream_pair_of(b.kind[0], b.kind[1], b.kind[2]);
+}
+
+void adjoint_tiling(BoxDesc &b, int min_items) {
+  const int cnz = (int)(b.cnp / ((int64_t)b.cnx * b.cny));
+  const int nu = NT * adj_upt(adjoint_pair_of(b)); // the pair kernel's columns per item
+  b.ant[0] = (b.cnx + TMAX - 1) / TMAX;
+  b.at[0] = (b.cnx + b.ant[0] - 1) / b.ant[0];
+  const int tymax = tile_ty(b.at[0], nu);
+  b.ant[1] = (b.cny + tymax - 1) / tymax;
+  b.at[1] = (b.cny + b.ant[1] - 1) / b.ant[1];
+  // coarse z per item: up to 48 (an item streams 2 (RHI - RLO) fine planes
+  // more than it owns), shorter (down to 8) until the box fills min_items
+  int maxz = 48;
+  const int64_t xy = (int64_t)b.ant[0] * b.ant[1] * b.ncomp;
+  while (maxz > 8 && xy * ((cnz + maxz - 1) / maxz) < min_items)
+    maxz /= 2;
+  const int n = (cnz + maxz - 1) / maxz;
+  b.at[2] = (cnz + n - 1) / n;
+  b.ant[2] = (cnz + b.at[2] - 1) / b.at[2];
+}
+
+int adjoint_level_grid(int pair) {
+  size_t smem = 0;
+  return adj_ready(pair, &smem) ? g_adj_grid[pair] : 0;
+}
+
+cudaError_t launch_prolong_adjoint_box(const BoxDesc &b0, int per_group, double *crse_bar,
                                        cudaStream_t s) {
   (void)per_group; // linear operators: per-group and per-variable agree
-  if (b.ncomp <= 0 || b.cnp <= 0)
+  if (b0.ncomp <= 0 || b0.cnp <= 0)
     return cudaSuccess;
-  const int pair = stream_pair_of(b.kind[0], b.kind[1], b.kind[2]);
+  const int pair = adjoint_pair_of(b0);
   size_t smem = 0;
-  AdjFn k = pair >= 0 ? adj_kernel(pair, &smem) : nullptr;
+  AdjFn k = adj_ready(pair, &smem);
   if (!k)
     return cudaErrorInvalidValue;
-  if (!g_adj_attr[pair]) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess)
-      return e;
-    int per_sm = 0, dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, smem);
-    g_adj_grid[pair] = sms * (per_sm > 0 ? per_sm : 1);
-    g_adj_attr[pair] = true;
-  }
-  const AdjTiling t = adj_tiling(b, g_adj_grid[pair]);
-  const int64_t n64 = (int64_t)t.ntx * t.nty * t.ntz * b.ncomp;
+  BoxDesc b = b0;
+  b.cbar = crse_bar;
+  adjoint_tiling(b, g_adj_grid[pair]);
+  const int64_t n64 = (int64_t)b.ant[0] * b.ant[1] * b.ant[2] * b.ncomp;
   if (n64 > INT32_MAX)
     return cudaErrorInvalidValue;
   const int n = (int)n64;
-  k<<<n < g_adj_grid[pair] ? n : g_adj_grid[pair], NT, smem, s>>>(b, t, crse_bar);
+  k<<<n < g_adj_grid[pair] ? n : g_adj_grid[pair], NT, smem, s>>>(b, nullptr, nullptr, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint_level(int pair, const BoxDesc *d_boxes, const TileRef *d_items,
+                                 int nitems, int grid, cudaStream_t s) {
+  if (nitems <= 0)
+    return cudaSuccess;
+  size_t smem = 0;
+  AdjFn k = adj_ready(pair, &smem);
+  if (!k)
+    return cudaErrorInvalidValue;
+  BoxDesc unused{};
+  k<<<grid < nitems ? grid : nitems, NT, smem, s>>>(unused, d_boxes, d_items, nitems);
   return cudaGetLastError();
 }
 

@@ -194,6 +194,10 @@ struct cx_level_plan {
   int group_off[kStrGroups + 1] = {};
   int group_grid[kStrGroups] = {};
   int64_t nfine = 0, bytes = 0;
+  // adjoint plan: execute computes crse = P^T fine for every box; coarse
+  // boxes whose region is empty are zeroed (pointer, bytes)
+  bool adjoint = false;
+  std::vector<std::pair<double *, size_t>> zero_boxes;
 };
 
 extern "C" {
@@ -394,10 +398,135 @@ int cx_level_plan_create(const cx_box_t *boxes, int nboxes, int per_group, cx_le
   return CX_OK;
 }
 
+int cx_level_plan_create_adjoint(const cx_box_t *boxes, int nboxes, int per_group,
+                                 cx_level_plan_t *out) {
+  if (!out || nboxes < 0 || (nboxes > 0 && !boxes))
+    return fail(CX_EINVAL, "invalid argument");
+  *out = nullptr;
+  if (int e = check_device())
+    return e;
+  cx_level_plan *p = new cx_level_plan;
+  p->per_group = per_group;
+  p->adjoint = true;
+  std::vector<int> ids;
+  for (int i = 0; i < nboxes; ++i) {
+    const cx_box_t &x = boxes[i];
+    BoxDesc b;
+    bool empty;
+    if (!x.crse && x.ncomp > 0) {
+      delete p;
+      return fail(CX_EINVAL, "box %d: null crse (the adjoint's output)", i);
+    }
+    if (int e = make_box(x.op, x.crse, x.crse_lo, x.crse_hi, x.fine, x.fine_lo, x.fine_hi,
+                         x.reg_lo, x.reg_hi, x.ncomp, per_group, &b, &empty)) {
+      delete p;
+      return fail(e, "box %d: %s", i, g_last_error.c_str());
+    }
+    if (empty) {
+      if (x.ncomp > 0 && box_ok(x.crse_lo, x.crse_hi))
+        p->zero_boxes.push_back({const_cast<double *>(x.crse),
+                                 sizeof(double) * box_points(x.crse_lo, x.crse_hi) * x.ncomp});
+      continue;
+    }
+    if (!op_separable(x.op, per_group) || adjoint_pair_of(b) < 0) {
+      delete p;
+      return fail(CX_EUNSUPPORTED, "box %d: adjoint of limited operators (ENO, minmod, linear "
+                                   "fallback) is not available", i);
+    }
+    b.cbar = const_cast<double *>(x.crse);
+    adjoint_tiling(b, 0);
+    if (b.ant[0] > INT16_MAX || b.ant[1] > INT16_MAX || b.ant[2] > INT16_MAX ||
+        x.ncomp > INT16_MAX) {
+      delete p;
+      return fail(CX_EINVAL, "box %d: too many tiles or components for a level plan", i);
+    }
+    int cl[3], ch[3];
+    cx_prolong_coarse_box(x.op, x.reg_lo, x.reg_hi, cl, ch);
+    p->nfine += box_points(x.reg_lo, x.reg_hi) * x.ncomp;
+    p->bytes += 8 * (box_points(cl, ch) + box_points(x.reg_lo, x.reg_hi)) * x.ncomp;
+    ids.push_back((int)p->boxes.size());
+    p->boxes.push_back(b);
+  }
+  // work items (box, x tile, y tile, z chunk, component) grouped by kernel
+  // instantiation and sorted by cost (fine planes x tile columns), largest
+  // first; equal costs keep the tiles of a box together, so neighbouring
+  // tiles stream at the same time and share their footprint halo in the L2
+  std::vector<std::pair<int64_t, TileRef>> keyed;
+  for (int id : ids) {
+    const BoxDesc &b = p->boxes[id];
+    const int cnz = (int)(b.cnp / ((int64_t)b.cnx * b.cny));
+    const int L = sep_rhi(b.kind[2]) - sep_rlo(b.kind[2]);
+    for (int c = 0; c < b.ncomp; ++c)
+      for (int tz = 0; tz < b.ant[2]; ++tz) {
+        const int nz = std::min(b.at[2], cnz - tz * b.at[2]);
+        for (int ty = 0; ty < b.ant[1]; ++ty)
+          for (int tx = 0; tx < b.ant[0]; ++tx) {
+            const int w = std::min(b.at[0], b.cnx - tx * b.at[0]);
+            const int h = std::min(b.at[1], b.cny - ty * b.at[1]);
+            keyed.push_back({(int64_t)(2 * (nz + L)) * w * h,
+                             TileRef{id, (int16_t)tx, (int16_t)ty, (int16_t)tz, (int16_t)c}});
+          }
+      }
+  }
+  auto group_of = [&](const TileRef &t) { return adjoint_pair_of(p->boxes[t.box]); };
+  std::stable_sort(keyed.begin(), keyed.end(),
+                   [&](const std::pair<int64_t, TileRef> &a, const std::pair<int64_t, TileRef> &b) {
+                     const int ga = group_of(a.second), gb = group_of(b.second);
+                     return ga != gb ? ga < gb : a.first > b.first;
+                   });
+  for (auto &k : keyed)
+    p->group_off[group_of(k.second) + 1]++;
+  for (int g = 0; g < kStrGroups; ++g)
+    p->group_off[g + 1] += p->group_off[g];
+  std::vector<TileRef> tiles;
+  tiles.reserve(keyed.size());
+  for (auto &k : keyed)
+    tiles.push_back(k.second);
+  if (tiles.size() > (size_t)INT32_MAX) {
+    delete p;
+    return fail(CX_EINVAL, "too many tiles");
+  }
+  p->nsep_tiles = (int)tiles.size();
+  cudaError_t e = cudaSuccess;
+  if (!p->boxes.empty())
+    e = cudaMalloc(&p->d_boxes, sizeof(BoxDesc) * p->boxes.size());
+  if (e == cudaSuccess && !tiles.empty())
+    e = cudaMalloc(&p->d_tiles, sizeof(TileRef) * tiles.size());
+  if (e == cudaSuccess && !p->boxes.empty())
+    e = cudaMemcpy(p->d_boxes, p->boxes.data(), sizeof(BoxDesc) * p->boxes.size(),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !tiles.empty())
+    e = cudaMemcpy(p->d_tiles, tiles.data(), sizeof(TileRef) * tiles.size(),
+                   cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cx_level_plan_destroy(p);
+    return fail(e == cudaErrorMemoryAllocation ? CX_ENOMEM : CX_ECUDA, "level plan: %s",
+                cudaGetErrorString(e));
+  }
+  for (int g = 0; g < kStrGroups; ++g)
+    p->group_grid[g] = p->group_off[g + 1] > p->group_off[g] ? adjoint_level_grid(g) : 0;
+  *out = p;
+  return CX_OK;
+}
+
 int cx_level_plan_execute(cx_level_plan_t p, cx_stream_t stream) {
   if (!p)
     return fail(CX_EINVAL, "null plan");
   cudaStream_t s = (cudaStream_t)stream;
+  if (p->adjoint) {
+    for (auto &z : p->zero_boxes)
+      if (int e = cuda_status(cudaMemsetAsync(z.first, 0, z.second, s), "memset"))
+        return e;
+    for (int g = 0; g < kStrGroups; ++g) {
+      const int n = p->group_off[g + 1] - p->group_off[g];
+      if (n > 0)
+        if (int e = cuda_status(launch_adjoint_level(g, p->d_boxes, p->d_tiles + p->group_off[g],
+                                                     n, p->group_grid[g], s),
+                                "adjoint level launch"))
+          return e;
+    }
+    return CX_OK;
+  }
   for (int g = 0; g < kStrGroups; ++g) {
     const int n = p->group_off[g + 1] - p->group_off[g];
     if (n > 0)
@@ -410,6 +539,19 @@ int cx_level_plan_execute(cx_level_plan_t p, cx_stream_t stream) {
     if (int e = cuda_status(launch_point_box(p->boxes[id], p->per_group, nullptr, nullptr, s),
                             "level launch (limited operators)"))
       return e;
+  return CX_OK;
+}
+
+int cx_check_device(void) {
+  if (int e = check_device())
+    return e;
+  if (int e = cuda_status(cudaDeviceSynchronize(), "device work"))
+    return e;
+  const int t = adjoint_take_timeout();
+  if (t < 0)
+    return fail(CX_ECUDA, "reading the device wait flag failed");
+  if (t > 0)
+    return fail(CX_ETIMEOUT, "a bounded device wait gave up (its results are not valid)");
   return CX_OK;
 }
 
@@ -513,10 +655,7 @@ int cx_prolong_adjoint_box(cx_op_t op, const double *crse, const int crse_lo[3],
           "memset");
     return CX_OK;
   }
-  bool linear = op_separable(op, per_group);
-  for (int d = 0; d < 3; ++d)
-    linear = linear && b.kind[d] != K_CC_MINMOD1;
-  if (!linear)
+  if (!op_separable(op, per_group) || adjoint_pair_of(b) < 0)
     return fail(CX_EUNSUPPORTED,
                 "adjoint of limited operators (ENO, minmod, linear fallback) is not available");
   return cuda_status(launch_prolong_adjoint_box(b, per_group, crse_bar, s), "adjoint launch");

@@ -36,6 +36,9 @@ struct BoxDesc {
   int xcw;            // streaming kernel: fine x per x chunk
   int npr;            // streaming kernel: pairs of fine y rows
   int upi;            // streaming kernel: units (columns) per item
+  double *cbar;       // adjoint: coarse output (P^T fine)
+  int at[3];          // adjoint: coarse tile extents in x, y; coarse z per item
+  int ant[3];         // adjoint: tiles per direction
 };
 
 // One unit of work of the level kernel: a tile of a box, one component.
@@ -82,5 +85,19 @@ cudaError_t launch_restrict_adjoint_box(int indextype, const double *crse_bar,
                                         cudaStream_t s);
 cudaError_t launch_prolong_adjoint_box(const BoxDesc &b, int per_group,
                                        double *crse_bar, cudaStream_t s);
+// Adjoint tiling of a box (cbar must be set by the caller); min_items > 0
+// shortens the z chunks of a box launched alone so that it spreads over at
+// least that many CTAs where it can.
+void adjoint_tiling(BoxDesc &b, int min_items);
+// Pair index of an operator whose adjoint has a kernel (linear separable),
+// else -1.
+int adjoint_pair_of(const BoxDesc &b);
+int adjoint_level_grid(int pair);
+// 1 if a bounded wait of the adjoint kernels gave up since the last call
+// (and clears the flag), 0 if not, -1 if the flag could not be read.
+int adjoint_take_timeout();
+cudaError_t launch_adjoint_level(int pair, const BoxDesc *d_boxes,
+                                 const TileRef *d_items, int nitems, int grid,
+                                 cudaStream_t s);
 
 } // namespace cxb

@@ -48,6 +48,12 @@ enum {
   CX_ENODEVICE = 6     /* no usable CUDA device */
 };
 
+/* Waits for all work on the current device; CX_ETIMEOUT if a kernel's
+ * bounded wait (on its own asynchronous copies) gave up since the last call,
+ * whose results are then not valid (the flag is cleared), CX_ECUDA on a CUDA
+ * error, CX_OK otherwise.  Kernels never wait without a bound. */
+int cx_check_device(void);
+
 /* Human-readable name of a status code. */
 const char *cx_status_string(int status);
 /* Text of the most recent failure on this thread ("" if none). */
@@ -140,6 +146,15 @@ int cx_level_plan_stats(cx_level_plan_t plan, int64_t *ntiles,
                         int64_t *nfine_points, int64_t *algorithmic_bytes);
 /* Frees the plan; the caller ensures no execution is still in flight. */
 int cx_level_plan_destroy(cx_level_plan_t plan);
+/* A level plan for the adjoint: executing it overwrites every box's crse
+ * array (whole coarse box, every component) with P^T of its fine array,
+ * reading the fine array only inside the region, as cx_prolong_adjoint_box
+ * does box by box; one persistent launch per stencil pair.  Validation is
+ * cx_prolong_box's; operators without a linear separable form (ENO, minmod,
+ * active linear fallback) give CX_EUNSUPPORTED.  Executed, destroyed and
+ * queried like any level plan. */
+int cx_level_plan_create_adjoint(const cx_box_t *boxes, int nboxes,
+                                 int per_group, cx_level_plan_t *out);
 
 /* ---------------------------------------------------------------------- */
 /* A whole level without allocating device memory                          */

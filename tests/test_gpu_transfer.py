@@ -225,3 +225,58 @@ def test_gpu_prolong_adjoint_tiled(dev, cx, typ, order, it):
     got = PTv.cpu().numpy()
     assert not np.any(np.isnan(got)), "coarse points left unwritten"
     np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12 * np.max(np.abs(want)))
+
+
+def test_gpu_adjoint_level_plan(dev, cx):
+    """cx_level_plan_create_adjoint: every box's coarse array becomes P^T of
+    its fine array, equal bit for bit to cx_prolong_adjoint_box (each coarse
+    plane is summed by one work item in fine-plane order, whatever the z
+    chunking) and to the oracle's transpose within roundoff; boxes with an
+    empty region are zeroed; limited operators are refused."""
+    rng = np.random.default_rng(11)
+    specs = [("interpolate", 5, 0), ("conservative", 1, 7), ("hermite", 3, 1), ("natural", 5, 6),
+             ("interpolate", 3, 7), ("ddf", 5, 3)]
+    boxes, per_box = [], []
+    for i in range(12):
+        typ, order, it = specs[i % len(specs)]
+        flo = tuple(int(v) for v in rng.integers(-6, 6, 3))
+        fhi = tuple(flo[d] + int(rng.integers(8, 70)) for d in range(3))
+        rlo = tuple(flo[d] + int(rng.integers(0, 3)) for d in range(3))
+        rhi = tuple(fhi[d] - int(rng.integers(0, 3)) for d in range(3))
+        if i == 11:
+            rhi = (rlo[0] - 1,) + rhi[1:]  # empty region
+        clo, chi = cx.coarse_box(typ, order, it, flo, fhi)
+        v = rng.standard_normal((2,) + box_shape(flo, fhi))
+        cbar = torch.full((2,) + box_shape(clo, chi), np.nan, dtype=torch.float64, device="cuda")
+        boxes.append(dict(op=cb.Op(typ, order, it), typ=typ, order=order, it=it, ncomp=2,
+                          crse=cbar, crse_lo=clo, crse_hi=chi, fine=cuda(v), fine_np=v,
+                          fine_lo=flo, fine_hi=fhi, reg_lo=rlo, reg_hi=rhi))
+    plan = cb.LevelPlan(boxes, adjoint=True)
+    plan.execute()
+    torch.cuda.synchronize()
+    for i, b in enumerate(boxes):
+        got = b["crse"].cpu().numpy()
+        one = torch.full_like(b["crse"], np.nan)
+        cb.prolong_adjoint_box(b["op"], b["crse"], b["crse_lo"], b["crse_hi"], b["fine"],
+                               b["fine_lo"], b["fine_hi"], b["reg_lo"], b["reg_hi"], 2, one)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(got, one.cpu().numpy(), err_msg=f"box {i} {b['typ']}")
+        want = np.zeros_like(got)
+        if i == 11:
+            assert np.all(got == 0)
+            continue
+        mask = region_mask(b["fine_lo"], b["fine_hi"], b["reg_lo"], b["reg_hi"])
+        cx.prolong_adjoint(b["typ"], b["order"], b["it"], 0, got, b["crse_lo"], b["crse_hi"],
+                           b["fine_np"] * mask, b["fine_lo"], b["fine_hi"], b["reg_lo"],
+                           b["reg_hi"], 2, want)
+        np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12 * np.max(np.abs(want)))
+    plan.close()
+    # no bounded device wait gave up
+    assert cb.lib().cx_check_device() == cb.CX_OK, cb.lib().cx_last_error()
+    lim = dict(boxes[0], op=cb.Op("minmod", 3, 7))
+    lim["crse_lo"], lim["crse_hi"] = cx.coarse_box("minmod", 3, 7, lim["fine_lo"], lim["fine_hi"])
+    lim["crse"] = torch.zeros((2,) + box_shape(lim["crse_lo"], lim["crse_hi"]),
+                              dtype=torch.float64, device="cuda")
+    with pytest.raises(cb.CxError) as e:
+        cb.LevelPlan([lim], adjoint=True)
+    assert e.value.status == cb.CX_EUNSUPPORTED
