@@ -18,7 +18,10 @@
 //          (TMA) copy of the row's 16-byte aligned middle, completing on the
 //          buffer's mbarrier (each row is placed in shared memory with the
 //          parity of its global address, so both ends of the copy are 16-byte
-//          aligned); the odd first/last point of a row takes an 8-byte copy;
+//          aligned); the odd first/last point of a row takes an 8-byte copy.
+//          The rows are dealt across the warps: a warp's bulk copies are
+//          issued one lane after the other, so spreading them shortens the
+//          issue;
 //   x^T    G(cx, fy) for the tile's coarse x and every footprint row, XB
 //          coarse x per task from a register window of the fine row, into
 //          shared memory (column major: the y taps of a column are adjacent);
@@ -102,15 +105,16 @@ template <class K> CXB_HD constexpr double wtap(int m) {
 }
 template <class K> constexpr int DK = K::RHI - K::RLO;
 
-// One CTA of NT threads per SM streams a tile of up to NT x UPT coarse
-// columns (at most TMAX per direction): large tiles keep the footprint halo,
-// loaded and transposed in x once more per tile, small (a 39 x 39 tile of
-// the order-5 stencils reads 1.27 fine points per point it owns).  A plane of
-// such a tile is several microseconds of work, so one plane prefetched ahead
-// covers the DRAM latency.
-constexpr int NT = 512;       // threads per CTA
+// A CTA of NT threads streams a tile of up to NT x UPT coarse columns (at
+// most TMAX per direction), two planes ahead; two CTAs per SM where the
+// shared memory allows (all but the order-7 pairs).  Measured on the
+// differentiated level (64 boxes of 32-96 coarse points per direction), this
+// beats one CTA of 512 threads with larger tiles (less footprint halo) and
+// one plane ahead: the time goes into waiting for the copies, and more CTAs
+// and planes in flight hide more of it.
+constexpr int NT = 256;       // threads per CTA
 constexpr int TMAX = 64;      // tile extent in x or y at most
-constexpr int DPF = 1;        // fine planes prefetched ahead
+constexpr int DPF = 2;        // fine planes prefetched ahead
 constexpr int NBUF = DPF + 1; // shared fine-plane ring
 constexpr int XB = 4;         // coarse x per x^T task
 
@@ -133,10 +137,8 @@ CXB_HD constexpr int max_fp(int dm, int nu, int what) {
   }
   return m;
 }
-// coarse columns per thread, as many as the registers hold next to the
-// ring of RHI - RLO + 1 partial sums per column: 4 up to spread 4, 3 for the
-// order-5 stencils, 2 for order 7
-CXB_HD constexpr int upt_of(int dm) { return dm <= 4 ? 4 : dm <= 6 ? 3 : 2; }
+// coarse columns per thread
+CXB_HD constexpr int upt_of(int) { return 2; }
 
 template <class KV, class KC> struct AdjPair {
   static constexpr int DM = DK<KV> > DK<KC> ? DK<KV> : DK<KC>;
@@ -148,6 +150,7 @@ template <class KV, class KC> struct AdjPair {
   // the last x^T window of a row may run 2 (XB - 1) points past the row
   static constexpr size_t SMEM = sizeof(double) * (size_t)(NBUF * FP + GP + 2 * XB);
   static_assert(SMEM + 1024 <= 227 * 1024, "shared memory per CTA");
+  static constexpr int OCC = SMEM + 2048 <= 113 * 1024 ? 2 : 1; // CTAs per SM
   static_assert(XTMAX <= 3, "x^T task registers");
 };
 
@@ -339,7 +342,7 @@ __device__ __forceinline__ bool adj_item(double *fbuf, double *gbuf, uint64_t *m
   // receives the bulk bytes; thread 0 arrives once every thread has issued)
   auto load = [&](int fz, int k) {
     double *S = fbuf + k * FP;
-    const int r = ay + tid; // footprint rows <= NT
+    const int r = ay + (tid & 31) * (NT / 32) + (tid >> 5); // footprint rows <= NT
     if (r <= by) {
       const int64_t rofs = org + (int64_t)fz * fplane + (int64_t)r * fnx; // (r, 0)
       const int par = (int)((fcomp8 + (uint64_t)rofs) & 1);
@@ -474,7 +477,7 @@ static_assert(BOX_WORDS <= NT, "one thread per descriptor word");
 // Level mode: items of a device work list (sorted by cost, the tiles of a box
 // together) strided over persistent CTAs.
 template <class KV, class KC>
-__global__ void __launch_bounds__(NT, 1)
+__global__ void __launch_bounds__(NT, AdjPair<KV, KC>::OCC)
     adjoint_kernel(const __grid_constant__ BoxDesc b, const BoxDesc *__restrict__ boxes,
                    const TileRef *__restrict__ items, int nitems) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
