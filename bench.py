@@ -27,6 +27,10 @@ One step = prolongation of every box and component of the level.  Reported:
              configuration (64 boxes, 32-96 coarse points per direction, 4
              variables), as level plans and one launch per box, and the
              adjoint/forward ratios
+  restriction  average_down of the conservative configuration (256^3 ->
+             128^3, 8 variables): time, GB/s and fraction of the HBM peak
+  limited    ENO order 3 and minmod (CCC, 64 boxes of 64^3 coarse cells, 5
+             variables) as level plans: fine points/s
   cpu_baseline  the reference operators compiled for the host
              (oracle/_ref, all host threads, OpenMP over boxes) on one
              component of every box
@@ -68,6 +72,10 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--adjoint-steps", type=int, default=3,
                    help="passes of the forward/adjoint comparison (0: skip)")
+    p.add_argument("--restrict-steps", type=int, default=5,
+                   help="passes of the restriction leg (0: skip)")
+    p.add_argument("--limited-steps", type=int, default=2,
+                   help="passes of the ENO / minmod leg (0: skip)")
     p.add_argument("--boxes", type=int, default=512, help="level512: number of boxes")
     p.add_argument("--ncomp", type=int, default=24, help="level512: variables per box")
     return p.parse_args()
@@ -165,6 +173,83 @@ def adjoint_leg(args, cb, torch, dev, max_over_ranks, barrier):
     plan_f.close()
     plan_a.close()
     del data
+    return out
+
+
+def restrict_leg(args, cb, torch, dev, max_over_ranks, barrier, peak):
+    """Restriction of the conservative configuration (cx_restrict_box): CCC
+    mean of the 2x2x2 children, fine cells 0..255 -> coarse region 0..127 of
+    the coarse box -3..130 (3 ghosts), 8 components.  Algorithmic bytes: 8 per
+    fine point read + 8 per coarse point written."""
+    nc = 8
+    flo, fhi = (0, 0, 0), (255, 255, 255)
+    clo, chi = (-3, -3, -3), (130, 130, 130)
+    rlo, rhi = (0, 0, 0), (127, 127, 127)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(args.seed + 2)
+    f = torch.randn((nc,) + box_shape(flo, fhi), dtype=torch.float64, device=dev, generator=gen)
+    c = torch.zeros((nc,) + box_shape(clo, chi), dtype=torch.float64, device=dev)
+    nbytes = 8 * nc * (npts(flo, fhi) + npts(rlo, rhi))
+
+    def step():
+        cb.restrict_box(7, f, flo, fhi, c, clo, chi, rlo, rhi, nc)
+
+    for _ in range(3):
+        step()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.restrict_steps):
+        step()
+    e1.record()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1)) / args.restrict_steps
+    gbs = nbytes / (ms / 1e3) / 1e9
+    del f, c
+    return {"workload": "restriction CCC (average_down), fine 256^3 -> coarse 128^3, 8 vars, "
+                        "one launch", "ms": ms, "bytes": nbytes, "achieved_gbs": gbs,
+            "frac_of_peak": gbs / peak}
+
+
+def limited_leg(args, cb, torch, dev, max_over_ranks, barrier):
+    """Limited operators of the shock configuration: ENO order 3 and minmod,
+    all directions cell centred, 64 boxes of 64^3 coarse cells (3 ghosts),
+    5 variables, a level plan each (the pointwise kernel).  The values are a
+    planar shock with jumps of 10x and Fourier modes on top, so the ENO shift
+    search and the minmod branches see both smooth and discontinuous data."""
+    nc, nb = 5, 64
+    flo, fhi = (0, 0, 0), (127, 127, 127)
+    out = {"workload": f"{nb} boxes, 64^3 coarse cells -> 128^3 fine, {nc} vars, CCC; level "
+                       "plans", "fine_points": nb * nc * npts(flo, fhi)}
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(args.seed + 4)
+    for typ, order in (("eno", 3), ("minmod", 1)):
+        op = cb.Op(typ, order, 7)
+        clo, chi = op.coarse_box(flo, fhi)
+        shape = (nc,) + box_shape(clo, chi)
+        z = torch.arange(shape[1], dtype=torch.float64, device=dev).view(1, -1, 1, 1)
+        boxes = []
+        for i in range(nb):
+            u = torch.randn(shape, dtype=torch.float64, device=dev, generator=gen) * 1e-2
+            u += torch.where(z > shape[1] * (0.3 + 0.4 * i / nb), 10.0, 1.0)
+            fine = torch.empty((nc,) + box_shape(flo, fhi), dtype=torch.float64, device=dev)
+            boxes.append(dict(op=op, ncomp=nc, crse=u, crse_lo=clo, crse_hi=chi, fine=fine,
+                              fine_lo=flo, fine_hi=fhi, reg_lo=flo, reg_hi=fhi))
+        plan = cb.LevelPlan(boxes)
+        for _ in range(2):
+            plan.execute()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.limited_steps):
+            plan.execute()
+        e1.record()
+        barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1)) / args.limited_steps
+        out[f"{typ}_ms"] = ms
+        out[f"{typ}_pts_per_s"] = out["fine_points"] / (ms / 1e3)
+        plan.close()
+        del boxes
     return out
 
 
@@ -466,8 +551,12 @@ def main():
 
     adjoint = adjoint_leg(args, cb, torch, dev, max_over_ranks, barrier) if args.adjoint_steps > 0 \
         else None
-
     peak, peak_src = measured_peaks()
+    restriction = (restrict_leg(args, cb, torch, dev, max_over_ranks, barrier, peak)
+                   if args.restrict_steps > 0 else None)
+    limited = (limited_leg(args, cb, torch, dev, max_over_ranks, barrier)
+               if args.limited_steps > 0 else None)
+
     # per GPU: the ranks' mean algorithmic bytes over the slowest rank's time
     mean_bytes = sum_over_ranks(alg_bytes, dev) / world
     achieved = mean_bytes / (ms_step / 1e3) / 1e9
@@ -499,6 +588,8 @@ def main():
                      "step_ms_min": min(per_step), "step_ms_max": max(per_step)},
         "clocks": clk,
         "adjoint": adjoint,
+        "restriction": restriction,
+        "limited": limited,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         lib, kind = cpu_lib()

@@ -69,6 +69,11 @@ void stream_tiling(BoxDesc &b, int min_items);
 cudaError_t launch_point_box(const BoxDesc &b, int per_group,
                              signed char *shifts, unsigned char *fallback,
                              cudaStream_t s);
+// The per-coarse-cell ENO kernel takes operators whose three directions are
+// CC ENO 2 without an active linear fallback (launch_point_box forwards).
+bool eno_cell_applies(const BoxDesc &b, int per_group);
+cudaError_t launch_eno_cell_box(const BoxDesc &b, int per_group, signed char *shifts,
+                                unsigned char *fallback, cudaStream_t s);
 cudaError_t launch_point_level(const BoxDesc *d_boxes, const TileRef *d_tiles,
                                int ntiles, int per_group, cudaStream_t s);
 

@@ -1,0 +1,285 @@
+// ENO prolongation per coarse cell, for operators whose three directions are
+// all CC ENO 2 and whose linear fallback is inactive (the "eno" family at
+// indextype 7, per var or per group).
+//
+// The reference chooses the stencil shift of every fine point
+// (CarpetX/src/prolongate_3d_rf2_impl.hxx:1415-1517 per var, 1857-1965 per
+// group): over the 27 shifts s (z outer, x inner) it takes
+//   dd(s) = (1 + sqrt(eps) |s|_1) * max(ddx, ddy, ddz),
+//   ddx = max over the 3 x 3 lines (j, k) around (cc + s) of
+//         |undivided difference in x at cc + s|, ddy and ddz alike,
+// and keeps the first minimum.  For ENO directions the line windows do not
+// depend on the fine offset, so the 8 children of a coarse cell share the
+// choice, and every term is a maximum of per-point |differences| D_d(p):
+//   max(ddx, ddy, ddz)(s) = M(cc + s),
+//   M(p) = max_d (max of D_d over the 3 x 3 window of p across d).
+// fmax is exact, so M and the choice equal the reference's bit for bit (for
+// NaN-free data).  The kernel computes D and M once per tile of coarse cells
+// in shared memory, searches the shift once per cell, and evaluates the 8
+// children with interp1d<CC,ENO,2> (impl.hxx:806-841) in call_stencil_3d's
+// order (x lines, then y, then z), sharing the x and y results between the
+// children: 38 1-D evaluations per cell instead of 8 x 13.
+#include "cx_internal.h"
+#include "cx_stencils.cuh"
+
+namespace cxb {
+namespace {
+
+constexpr int ET = 8;           // coarse cells per tile edge
+constexpr int EW = ET + 4;      // window edge: tile plus 2 cells each side
+constexpr int EW3 = EW * EW * EW;
+constexpr int ENT = 256;        // threads per CTA
+constexpr int ECPT = ET * ET * ET / ENT; // cells per thread
+
+struct EnoShared {
+  double c[EW3];    // coarse window of one component
+  double d[3][EW3]; // |undivided differences| per direction (max over the block's components)
+  double t[EW3];    // window maximum along the first axis
+  double m[EW3];    // M(p)
+};
+
+__device__ __forceinline__ int widx(int i, int j, int k) { return (k * EW + j) * EW + i; }
+
+// undivided_difference_1d<CC,ENO,2> (impl.hxx:751-773): -2 c0 + (c- + c+).
+__device__ __forceinline__ double undiv2(double cm, double c0, double cp) {
+  return fadd(fmul(-2.0, c0), fmul(1.0, fadd(cm, cp)));
+}
+
+// The three coefficients of interp1d<CC,ENO,2> for (shift, off), in tap order:
+// row m = shift + 1 (off 0) or 1 - shift (off 1), reversed for off 1.
+__device__ __forceinline__ void eno2_coeffs(int shift, int off, double w[3]) {
+  const int m = off == 0 ? shift + 1 : 1 - shift;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const int j = off == 0 ? i : 2 - i;
+    w[i] = m == 0 ? cc_eno2_c(0, j) : m == 1 ? cc_eno2_c(1, j) : cc_eno2_c(2, j);
+  }
+}
+// The reference's sum from 0 (impl.hxx:820-841), taps at shift - 1 .. shift + 1.
+__device__ __forceinline__ double eno2_apply(const double w[3], double t0, double t1, double t2) {
+  return fadd(fadd(fadd(0.0, fmul(w[0], t0)), fmul(w[1], t1)), fmul(w[2], t2));
+}
+
+struct EnoTiling {
+  int clo[3];   // first coarse cell of the region (rlo >> 1)
+  int nt[3];    // tiles per direction
+  int nblk;     // component blocks: ncomp (per var) or 1 (per group)
+};
+
+__global__ void __launch_bounds__(ENT, 2)
+    eno_cell_kernel(const __grid_constant__ BoxDesc b, const EnoTiling t, int per_group,
+                    signed char *shifts, unsigned char *fallback) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  EnoShared &sh = *reinterpret_cast<EnoShared *>(smem_raw);
+  const int tid = threadIdx.x;
+  const int rnx = b.rhi[0] - b.rlo[0] + 1, rny = b.rhi[1] - b.rlo[1] + 1;
+  const int64_t rnp = (int64_t)rnx * rny * (b.rhi[2] - b.rlo[2] + 1);
+  const int64_t cplane = (int64_t)b.cnx * b.cny, fplane = (int64_t)b.fnx * b.fny;
+  const int ntiles = t.nt[0] * t.nt[1] * t.nt[2];
+  for (int item = blockIdx.x; item < ntiles * t.nblk; item += gridDim.x) {
+    const int tile = item % ntiles, blk = item / ntiles;
+    const int tx = tile % t.nt[0], ty = (tile / t.nt[0]) % t.nt[1], tz = tile / (t.nt[0] * t.nt[1]);
+    // window origin (coarse index of local 0) and the block's components
+    const int o0 = t.clo[0] + tx * ET - 2, o1 = t.clo[1] + ty * ET - 2, o2 = t.clo[2] + tz * ET - 2;
+    const int c0 = per_group ? 0 : blk, c1 = per_group ? b.ncomp : blk + 1;
+
+    // load the window of component comp: the coarse points the operator
+    // reads (the rest of the window reaches only cells outside the region)
+    auto load = [&](int comp) {
+      const double *cb = b.crse + comp * b.cnp;
+      for (int e = tid; e < EW3; e += ENT) {
+        const int i = e % EW, j = (e / EW) % EW, k = e / (EW * EW);
+        const int gi = o0 + i, gj = o1 + j, gk = o2 + k;
+        if (gi >= b.nlo[0] && gi <= b.nhi[0] && gj >= b.nlo[1] && gj <= b.nhi[1] &&
+            gk >= b.nlo[2] && gk <= b.nhi[2])
+          sh.c[e] = __ldg(cb + (gi - b.clo[0]) + (int64_t)b.cnx * (gj - b.clo[1]) +
+                          cplane * (gk - b.clo[2]));
+      }
+    };
+
+    // D_d = max over the block's components of |undivided difference in d|
+    for (int e = tid; e < 3 * EW3; e += ENT)
+      (&sh.d[0][0])[e] = 0.0;
+    for (int comp = c0; comp < c1; ++comp) {
+      __syncthreads();
+      load(comp);
+      __syncthreads();
+      for (int e = tid; e < EW3; e += ENT) {
+        const int i = e % EW, j = (e / EW) % EW, k = e / (EW * EW);
+        if (i >= 1 && i <= EW - 2)
+          sh.d[0][e] = fmax(sh.d[0][e], fabs(undiv2(sh.c[e - 1], sh.c[e], sh.c[e + 1])));
+        if (j >= 1 && j <= EW - 2)
+          sh.d[1][e] = fmax(sh.d[1][e], fabs(undiv2(sh.c[e - EW], sh.c[e], sh.c[e + EW])));
+        if (k >= 1 && k <= EW - 2)
+          sh.d[2][e] = fmax(sh.d[2][e], fabs(undiv2(sh.c[e - EW * EW], sh.c[e], sh.c[e + EW * EW])));
+      }
+    }
+    __syncthreads();
+    // M(p) = max over d of the 3 x 3 window maximum of D_d across d, for
+    // p in [1, EW - 2]^3 (the shifted cells the search visits)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      // window axes of direction d: (y, z) for x, (x, z) for y, (x, y) for z
+      const int SA_d = d == 0 ? EW : 1;
+      const int SB_d = d == 2 ? EW : EW * EW;
+      for (int e = tid; e < EW3; e += ENT) {
+        const int i = e % EW, j = (e / EW) % EW, k = e / (EW * EW);
+        const int a = d == 0 ? j : i;
+        if (a >= 1 && a <= EW - 2)
+          sh.t[e] = fmax(fmax(sh.d[d][e - SA_d], sh.d[d][e]), sh.d[d][e + SA_d]);
+      }
+      __syncthreads();
+      for (int e = tid; e < EW3; e += ENT) {
+        const int i = e % EW, j = (e / EW) % EW, k = e / (EW * EW);
+        if (i >= 1 && i <= EW - 2 && j >= 1 && j <= EW - 2 && k >= 1 && k <= EW - 2) {
+          const double w = fmax(fmax(sh.t[e - SB_d], sh.t[e]), sh.t[e + SB_d]);
+          sh.m[e] = d == 0 ? w : fmax(sh.m[e], w);
+        }
+      }
+      __syncthreads();
+    }
+
+    // shift search per cell: first minimum in the reference's order
+    int cell[ECPT], shx[ECPT], shy[ECPT], shz[ECPT];
+#pragma unroll
+    for (int q = 0; q < ECPT; ++q) {
+      const int u = tid + q * ENT;
+      const int ci = u % ET, cj = (u / ET) % ET, ck = u / (ET * ET);
+      cell[q] = widx(ci + 2, cj + 2, ck + 2);
+      double min_dd = __longlong_as_double(0x7ff0000000000000LL); // +inf
+      int bx = 0, by = 0, bz = 0;
+      for (int sk = -1; sk <= 1; ++sk)
+        for (int sj = -1; sj <= 1; ++sj)
+#pragma unroll
+          for (int si = -1; si <= 1; ++si) {
+            // 1 + sqrt(DBL_EPSILON) * |s|_1, sqrt(2^-52) = 2^-26 exactly
+            const double pen = fadd(1.0, fmul(0x1p-26, (double)(abs(si) + abs(sj) + abs(sk))));
+            const double dd = fmul(pen, sh.m[cell[q] + si + EW * sj + EW * EW * sk]);
+            if (dd < min_dd) {
+              min_dd = dd;
+              bx = si;
+              by = sj;
+              bz = sk;
+            }
+          }
+      shx[q] = bx;
+      shy[q] = by;
+      shz[q] = bz;
+    }
+
+    // evaluate the children of every cell, component by component
+    for (int comp = c0; comp < c1; ++comp) {
+      if (c1 - c0 > 1 || comp != c1 - 1) { // the window holds the last component loaded
+        __syncthreads();
+        load(comp);
+        __syncthreads();
+      }
+      double *fb = b.fine + comp * b.fnp;
+#pragma unroll 1
+      for (int q = 0; q < ECPT; ++q) {
+        const int u = tid + q * ENT;
+        const int ci = u % ET, cj = (u / ET) % ET, ck = u / (ET * ET);
+        const int gi = o0 + 2 + ci, gj = o1 + 2 + cj, gk = o2 + 2 + ck; // coarse cell
+        const int f0x = 2 * gi, f0y = 2 * gj, f0z = 2 * gk;
+        if (f0x + 1 < b.rlo[0] || f0x > b.rhi[0] || f0y + 1 < b.rlo[1] || f0y > b.rhi[1] ||
+            f0z + 1 < b.rlo[2] || f0z > b.rhi[2])
+          continue; // no child in the region
+        double wy[2][3], wz[2][3];
+#pragma unroll
+        for (int o = 0; o < 2; ++o) {
+          eno2_coeffs(shy[q], o, wy[o]);
+          eno2_coeffs(shz[q], o, wz[o]);
+        }
+        // x lines at y = cj + shy - 1 + a, z = ck + shz - 1 + g
+        const int base = cell[q] + (shx[q] - 1) + EW * (shy[q] - 1) + EW * EW * (shz[q] - 1);
+#pragma unroll 1
+        for (int ox = 0; ox < 2; ++ox) {
+          double wx[3];
+          eno2_coeffs(shx[q], ox, wx);
+          double X[3][3];
+#pragma unroll
+          for (int g = 0; g < 3; ++g)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+              const double *v = sh.c + base + EW * a + EW * EW * g;
+              X[a][g] = eno2_apply(wx, v[0], v[1], v[2]);
+            }
+#pragma unroll
+          for (int oy = 0; oy < 2; ++oy) {
+            double Y[3];
+#pragma unroll
+            for (int g = 0; g < 3; ++g)
+              Y[g] = eno2_apply(wy[oy], X[0][g], X[1][g], X[2][g]);
+#pragma unroll
+            for (int oz = 0; oz < 2; ++oz) {
+              const int fx = f0x + ox, fy = f0y + oy, fz = f0z + oz;
+              if (fx < b.rlo[0] || fx > b.rhi[0] || fy < b.rlo[1] || fy > b.rhi[1] ||
+                  fz < b.rlo[2] || fz > b.rhi[2])
+                continue;
+              const double r = eno2_apply(wz[oz], Y[0], Y[1], Y[2]);
+              fb[(fx - b.flo[0]) + (int64_t)b.fnx * (fy - b.flo[1]) + fplane * (fz - b.flo[2])] = r;
+              if (comp == c0 && (shifts || fallback)) {
+                const int64_t ridx = (fx - b.rlo[0]) + (int64_t)rnx * ((fy - b.rlo[1]) +
+                                                                      (int64_t)rny * (fz - b.rlo[2]));
+                if (shifts) {
+                  signed char *sp = shifts + 3 * (blk * rnp + ridx);
+                  sp[0] = (signed char)shx[q];
+                  sp[1] = (signed char)shy[q];
+                  sp[2] = (signed char)shz[q];
+                }
+                if (fallback)
+                  fallback[blk * rnp + ridx] = 0;
+              }
+            }
+          }
+        }
+      }
+    }
+    __syncthreads(); // the next item reuses the shared arrays
+  }
+}
+
+bool g_eno_attr = false;
+int g_eno_grid = 0;
+
+} // namespace
+
+bool eno_cell_applies(const BoxDesc &b, int per_group) {
+  return b.kind[0] == K_CC_ENO2 && b.kind[1] == K_CC_ENO2 && b.kind[2] == K_CC_ENO2 &&
+         !op_fb_active(b.op, per_group);
+}
+
+cudaError_t launch_eno_cell_box(const BoxDesc &b, int per_group, signed char *shifts,
+                                unsigned char *fallback, cudaStream_t s) {
+  if (b.ncomp <= 0)
+    return cudaSuccess;
+  EnoTiling t;
+  for (int d = 0; d < 3; ++d) {
+    if (b.rhi[d] < b.rlo[d])
+      return cudaSuccess;
+    t.clo[d] = b.rlo[d] >> 1;
+    const int ncell = (b.rhi[d] >> 1) - t.clo[d] + 1;
+    t.nt[d] = (ncell + ET - 1) / ET;
+  }
+  t.nblk = per_group ? 1 : b.ncomp;
+  const int64_t n = (int64_t)t.nt[0] * t.nt[1] * t.nt[2] * t.nblk;
+  if (n > INT32_MAX)
+    return cudaErrorInvalidValue;
+  if (!g_eno_attr) {
+    cudaError_t e = cudaFuncSetAttribute(eno_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(EnoShared));
+    if (e != cudaSuccess)
+      return e;
+    int per_sm = 0, dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eno_cell_kernel, ENT, sizeof(EnoShared));
+    g_eno_grid = sms * (per_sm > 0 ? per_sm : 1);
+    g_eno_attr = true;
+  }
+  const int grid = n < g_eno_grid ? (int)n : g_eno_grid;
+  eno_cell_kernel<<<grid, ENT, sizeof(EnoShared), s>>>(b, t, per_group, shifts, fallback);
+  return cudaGetLastError();
+}
+
+} // namespace cxb
