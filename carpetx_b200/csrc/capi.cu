@@ -655,9 +655,8 @@ int cx_prolong_adjoint_box(cx_op_t op, const double *crse, const int crse_lo[3],
           "memset");
     return CX_OK;
   }
-  if (!op_separable(op, per_group) || adjoint_pair_of(b) < 0)
-    return fail(CX_EUNSUPPORTED,
-                "adjoint of limited operators (ENO, minmod, linear fallback) is not available");
+  if (!op_separable(op, per_group) || adjoint_pair_of(b) < 0) // ENO, minmod, fallback
+    return cuda_status(launch_point_adjoint_box(b, per_group, crse_bar, s), "adjoint launch");
   return cuda_status(launch_prolong_adjoint_box(b, per_group, crse_bar, s), "adjoint launch");
 }
 

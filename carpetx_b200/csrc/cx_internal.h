@@ -90,6 +90,10 @@ cudaError_t launch_restrict_adjoint_box(int indextype, const double *crse_bar,
                                         cudaStream_t s);
 cudaError_t launch_prolong_adjoint_box(const BoxDesc &b, int per_group,
                                        double *crse_bar, cudaStream_t s);
+// Adjoint of the limited operators (ENO, minmod, active linear fallback):
+// decision pass into stream-ordered scratch, then a gather per coarse point.
+cudaError_t launch_point_adjoint_box(const BoxDesc &b, int per_group,
+                                     double *crse_bar, cudaStream_t s);
 // Adjoint tiling of a box (cbar must be set by the caller); min_items > 0
 // shortens the z chunks of a box launched alone so that it spreads over at
 // least that many CTAs where it can.

@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(ENT, 2)
         load(comp);
         __syncthreads();
       }
-      double *fb = b.fine + comp * b.fnp;
+      double *fb = b.fine ? b.fine + comp * b.fnp : nullptr;
 #pragma unroll 1
       for (int q = 0; q < ECPT; ++q) {
         const int u = tid + q * ENT;
@@ -217,7 +217,8 @@ __global__ void __launch_bounds__(ENT, 2)
                   fz < b.rlo[2] || fz > b.rhi[2])
                 continue;
               const double r = eno2_apply(wz[oz], Y[0], Y[1], Y[2]);
-              fb[(fx - b.flo[0]) + (int64_t)b.fnx * (fy - b.flo[1]) + fplane * (fz - b.flo[2])] = r;
+              if (fb) // null: decisions only (the adjoint's decision pass)
+                fb[(fx - b.flo[0]) + (int64_t)b.fnx * (fy - b.flo[1]) + fplane * (fz - b.flo[2])] = r;
               if (comp == c0 && (shifts || fallback)) {
                 const int64_t ridx = (fx - b.rlo[0]) + (int64_t)rnx * ((fy - b.rlo[1]) +
                                                                       (int64_t)rny * (fz - b.rlo[2]));

@@ -229,15 +229,199 @@ __global__ void __launch_bounds__(256)
   const int64_t fidx = (ifine[0] - b.flo[0]) +
                        (int64_t)b.fnx * ((ifine[1] - b.flo[1]) + (int64_t)b.fny * (ifine[2] - b.flo[2]));
   const int zero3[3] = {0, 0, 0};
-  for (int comp = c0; comp < c1; ++comp) {
-    const double res = need ? eval3d(lin, zero3, off, c, comp, ic) : vals[comp - c0];
-    b.fine[comp * b.fnp + fidx] = res;
-  }
+  if (b.fine) // null: decisions only (the adjoint's decision pass)
+    for (int comp = c0; comp < c1; ++comp) {
+      const double res = need ? eval3d(lin, zero3, off, c, comp, ic) : vals[comp - c0];
+      b.fine[comp * b.fnp + fidx] = res;
+    }
   if (shifts)
     for (int d = 0; d < 3; ++d)
       shifts[3 * (blk * rnp + idx) + d] = (signed char)shift[d];
   if (fallback)
     fallback[blk * rnp + idx] = need ? 1 : 0;
+}
+
+
+// ---------------------------------------------------------------------------
+// Adjoint of the limited operators (ENO, minmod, linear fallback), gather
+// form: P^T linearised at the forward input, as the transpose of the map each
+// fine point applies (the reference's choices treated as locally constant).
+// A decision pass (the forward kernels with value stores off) writes every
+// region point's ENO shift and fallback flag; here one thread per coarse
+// point c (per component) sums, over the fine points f whose stencil can
+// reach c, w(f, c) * fine_bar(f) in a fixed order (no atomics):
+//   w(f, c) = wz(k) wy(j; k) wx(i; j, k),  (i, j, k) = c - cell(f),
+// with each 1-D weight that of the kind f applies in that direction (its
+// fallback kind if it fell back, with shift 0).  For the linear kinds the
+// weights are constants of (kind, shift, off), tabulated per CTA by
+// evaluating the stencil on unit vectors (the reference's arithmetic); a
+// minmod direction's weights depend on the values it reads, which are
+// re-evaluated (x lines from coarse data, y from the x results).
+
+// 1-D weights of a minmod application at line values v[-1..1] (impl.hxx:
+// 859-877 differentiated; fmin keeps |dm| on ties).
+__device__ __forceinline__ void minmod_weights(int off, const double *v, double w[3]) {
+  const double dm = v[0] - v[-1], dp = v[1] - v[0];
+  const double sgn = off == 0 ? -1.0 : 1.0;
+  w[0] = 0.0;
+  w[1] = 1.0;
+  w[2] = 0.0;
+  const double f = copysign(0.125, dm) + copysign(0.125, dp);
+  if (f != 0.0) {
+    if (fabs(dm) <= fabs(dp)) {
+      w[1] += sgn * 0.25;
+      w[0] -= sgn * 0.25;
+    } else {
+      w[2] += sgn * 0.25;
+      w[1] -= sgn * 0.25;
+    }
+  }
+}
+
+constexpr int AT_NT = 128; // threads per CTA
+
+// weight table: [direction][0: kind, 1: fallback kind][shift + 1][off][o + 4]
+struct AdjTable {
+  double w[3][2][3][2][9];
+};
+
+__global__ void __launch_bounds__(AT_NT)
+    adjoint_point_kernel(const BoxDesc b, int per_group, const signed char *shifts,
+                         const unsigned char *fallback, double *crse_bar) {
+  __shared__ AdjTable tab;
+  int kind[3], lin[3], lo[3], hi[3];
+  bool mm[3], mml[3];
+  for (int d = 0; d < 3; ++d) {
+    kind[d] = b.kind[d];
+    const KindInfo ki = kind_info(kind[d]);
+    lin[d] = (ki.intp == CONS || (!per_group && ki.intp == ENO)) ? K_CC_CONS1 : kind[d];
+    mm[d] = kind[d] == K_CC_MINMOD1;
+    mml[d] = lin[d] == K_CC_MINMOD1;
+    // coarse offsets any fine point may read (ENO search window, both parities)
+    int a, c, a1, c1;
+    read_range(kind[d], 0, &a, &c);
+    read_range(kind[d], 1, &a1, &c1);
+    lo[d] = min(a, a1);
+    hi[d] = max(c, c1);
+  }
+  // tabulate the linear weights (unused entries stay 0)
+  for (int e = threadIdx.x; e < 3 * 2 * 3 * 2; e += blockDim.x) {
+    const int off = e % 2, sh = (e / 2) % 3 - 1, which = (e / 6) % 2, d = e / 12;
+    const int k = which ? lin[d] : kind[d];
+    double *w = tab.w[d][which][sh + 1][off];
+    for (int o = 0; o < 9; ++o)
+      w[o] = 0.0;
+    if (k == K_CC_MINMOD1 || (sh != 0 && k != K_CC_ENO2))
+      continue;
+    int r[2];
+    radius(k, sh, off, r);
+    for (int o = r[0]; o <= r[1]; ++o) {
+      double unit[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      unit[o + 4] = 1.0;
+      w[o + 4] = ap_rt(k, sh, off, unit + 4);
+    }
+  }
+  __syncthreads();
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= b.cnp)
+    return;
+  const int blk = blockIdx.y; // component (per var) or 0 (per group)
+  const int c0 = per_group ? 0 : blk, c1 = per_group ? b.ncomp : blk + 1;
+  const int cz = b.clo[2] + (int)(idx / ((int64_t)b.cnx * b.cny));
+  const int cy = b.clo[1] + (int)((idx / b.cnx) % b.cny);
+  const int cx = b.clo[0] + (int)(idx % b.cnx);
+  const int cc[3] = {cx, cy, cz};
+  const int rnx = b.rhi[0] - b.rlo[0] + 1, rny = b.rhi[1] - b.rlo[1] + 1;
+  const int64_t rnp = (int64_t)rnx * rny * (b.rhi[2] - b.rlo[2] + 1);
+  const int64_t fplane = (int64_t)b.fnx * b.fny;
+  Coarse crs;
+  crs.p = b.crse;
+  crs.np = b.cnp;
+  crs.nx = b.cnx;
+  crs.ny = b.cny;
+  for (int d = 0; d < 3; ++d)
+    crs.lo[d] = b.clo[d];
+  for (int comp = c0; comp < c1; ++comp) {
+    double acc = 0.0;
+    for (int kz = cz - hi[2]; kz <= cz - lo[2]; ++kz)
+      for (int ky = cy - hi[1]; ky <= cy - lo[1]; ++ky)
+        for (int kx = cx - hi[0]; kx <= cx - lo[0]; ++kx)
+          for (int o8 = 0; o8 < 8; ++o8) {
+            const int ic[3] = {kx, ky, kz};
+            const int off[3] = {o8 & 1, (o8 >> 1) & 1, o8 >> 2};
+            const int f[3] = {2 * kx + off[0], 2 * ky + off[1], 2 * kz + off[2]};
+            if (f[0] < b.rlo[0] || f[0] > b.rhi[0] || f[1] < b.rlo[1] || f[1] > b.rhi[1] ||
+                f[2] < b.rlo[2] || f[2] > b.rhi[2])
+              continue;
+            const int64_t ridx = (f[0] - b.rlo[0]) + (int64_t)rnx * ((f[1] - b.rlo[1]) +
+                                                                    (int64_t)rny * (f[2] - b.rlo[2]));
+            int sh[3] = {0, 0, 0};
+            int fbk = 0;
+            if (shifts)
+              for (int d = 0; d < 3; ++d)
+                sh[d] = shifts[3 * (blk * rnp + ridx) + d];
+            if (fallback)
+              fbk = fallback[blk * rnp + ridx];
+            int k[3], o[3], r[3][2];
+            bool inside = true, anymm = false;
+            for (int d = 0; d < 3; ++d) {
+              if (fbk)
+                sh[d] = 0;
+              k[d] = fbk ? lin[d] : kind[d];
+              o[d] = cc[d] - ic[d];
+              radius(k[d], sh[d], off[d], r[d]);
+              inside = inside && o[d] >= r[d][0] && o[d] <= r[d][1];
+              anymm = anymm || (fbk ? mml[d] : mm[d]);
+            }
+            if (!inside)
+              continue;
+            double w;
+            if (!anymm) {
+              w = tab.w[0][fbk][sh[0] + 1][off[0]][o[0] + 4] *
+                  tab.w[1][fbk][sh[1] + 1][off[1]][o[1] + 4] *
+                  tab.w[2][fbk][sh[2] + 1][off[2]][o[2] + 4];
+            } else {
+              // re-evaluate the passes of f's stencil (call_stencil_3d order)
+              double X[9][9], Y[9];
+              for (int dk = r[2][0]; dk <= r[2][1]; ++dk) {
+                for (int dj = r[1][0]; dj <= r[1][1]; ++dj) {
+                  double v[9];
+                  for (int di = r[0][0]; di <= r[0][1]; ++di)
+                    v[di + 4] = crs(comp, ic[0] + di, ic[1] + dj, ic[2] + dk);
+                  X[dk + 4][dj + 4] = ap_rt(k[0], sh[0], off[0], v + 4);
+                }
+                Y[dk + 4] = ap_rt(k[1], sh[1], off[1], X[dk + 4] + 4);
+              }
+              double wz, wy, wx, t[3];
+              if (k[2] == K_CC_MINMOD1) {
+                minmod_weights(off[2], Y + 4, t);
+                wz = t[o[2] + 1];
+              } else {
+                wz = tab.w[2][fbk][sh[2] + 1][off[2]][o[2] + 4];
+              }
+              if (k[1] == K_CC_MINMOD1) {
+                minmod_weights(off[1], X[o[2] + 4] + 4, t);
+                wy = t[o[1] + 1];
+              } else {
+                wy = tab.w[1][fbk][sh[1] + 1][off[1]][o[1] + 4];
+              }
+              if (k[0] == K_CC_MINMOD1) {
+                double v[3];
+                for (int di = -1; di <= 1; ++di)
+                  v[di + 1] = crs(comp, ic[0] + di, ic[1] + o[1], ic[2] + o[2]);
+                minmod_weights(off[0], v + 1, t);
+                wx = t[o[0] + 1];
+              } else {
+                wx = tab.w[0][fbk][sh[0] + 1][off[0]][o[0] + 4];
+              }
+              w = wz * wy * wx;
+            }
+            acc = fma(w, b.fine[comp * b.fnp + (f[0] - b.flo[0]) + (int64_t)b.fnx * (f[1] - b.flo[1]) +
+                                fplane * (f[2] - b.flo[2])],
+                      acc);
+          }
+    crse_bar[comp * b.cnp + idx] = acc;
+  }
 }
 
 } // namespace
@@ -256,6 +440,53 @@ cudaError_t launch_point_box(const BoxDesc &b, int per_group, signed char *shift
   dim3 grid((unsigned)nblk, per_group ? 1 : b.ncomp);
   point_box_kernel<<<grid, 256, 0, s>>>(b, per_group, shifts, fallback);
   return cudaGetLastError();
+}
+
+// Adjoint of a limited operator on one box: decision pass into stream-ordered
+// scratch (the ENO shift and fallback flag of every region point, recomputed
+// from crse), then the gather.  fine in b holds fine_bar.
+cudaError_t launch_point_adjoint_box(const BoxDesc &b, int per_group, double *crse_bar,
+                                     cudaStream_t s) {
+  if (b.ncomp <= 0 || b.cnp <= 0)
+    return cudaSuccess;
+  const int64_t rnp = (int64_t)(b.rhi[0] - b.rlo[0] + 1) * (b.rhi[1] - b.rlo[1] + 1) *
+                      (b.rhi[2] - b.rlo[2] + 1);
+  const int nblk = per_group ? 1 : b.ncomp;
+  bool eno = false;
+  for (int d = 0; d < 3; ++d)
+    eno = eno || b.kind[d] == K_CC_ENO2;
+  const bool decide = eno || op_fb_active(b.op, per_group);
+  signed char *sh = nullptr;
+  unsigned char *fb = nullptr;
+  void *scratch = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (decide && rnp > 0) {
+    const size_t n = (size_t)rnp * nblk;
+    e = cudaMallocAsync(&scratch, 4 * n, s);
+    if (e != cudaSuccess)
+      return e;
+    sh = static_cast<signed char *>(scratch);
+    fb = reinterpret_cast<unsigned char *>(sh + 3 * n);
+    BoxDesc d = b;
+    d.fine = nullptr; // decisions only
+    e = launch_point_box(d, per_group, sh, fb, s);
+  }
+  if (e == cudaSuccess) {
+    const int64_t nb = (b.cnp + AT_NT - 1) / AT_NT;
+    if (nb > INT32_MAX) {
+      e = cudaErrorInvalidValue;
+    } else {
+      adjoint_point_kernel<<<dim3((unsigned)nb, nblk), AT_NT, 0, s>>>(b, per_group, sh, fb,
+                                                                       crse_bar);
+      e = cudaGetLastError();
+    }
+  }
+  if (scratch) {
+    const cudaError_t e2 = cudaFreeAsync(scratch, s);
+    if (e == cudaSuccess)
+      e = e2;
+  }
+  return e;
 }
 
 } // namespace cxb

@@ -203,7 +203,10 @@ int cx_restrict_box(int indextype, const double *fine, const int fine_lo[3],
 /* crse_bar = P^T fine_bar, with P the prolongation of cx_prolong_box
  * linearised at crse (ENO shift, minmod branch and linear-fallback choice
  * recomputed from crse).  crse_bar is overwritten over the whole coarse
- * box (zero where no region point reads).  Gather form, no atomics. */
+ * box (zero where no region point reads).  Gather form, no atomics.  The
+ * linear separable operators stream; the limited ones (ENO, minmod, active
+ * linear fallback) take a decision pass and a gather per coarse point, with
+ * stream-ordered scratch of 4 bytes per region point (cudaMallocAsync). */
 int cx_prolong_adjoint_box(cx_op_t op, const double *crse,
                            const int crse_lo[3], const int crse_hi[3],
                            const double *fine_bar, const int fine_lo[3],

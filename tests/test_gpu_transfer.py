@@ -280,3 +280,39 @@ def test_gpu_adjoint_level_plan(dev, cx):
     with pytest.raises(cb.CxError) as e:
         cb.LevelPlan([lim], adjoint=True)
     assert e.value.status == cb.CX_EUNSUPPORTED
+
+
+@pytest.mark.parametrize("typ,order,it", [("eno", 3, 7), ("eno", 5, 1), ("minmod", 1, 7),
+                                          ("minmod", 3, 3), ("poly-cons3lfb", 3, 7),
+                                          ("poly-eno3lfb", 5, 6), ("poly-cons3lfb", 5, 0)])
+@pytest.mark.parametrize("pg", [0, 1])
+def test_gpu_prolong_adjoint_limited(dev, cx, typ, order, it, pg):
+    """Adjoint of the limited operators, linearised at the coarse input (ENO
+    shift, minmod branch, fallback choice recomputed): against the oracle's
+    transpose, and the dot-product identity <P(u), v> = <u, P'(u)^T v>, exact
+    for these piecewise-linear maps."""
+    from helpers import random_case
+    rng = np.random.default_rng(order * 100 + it * 10 + pg)
+    for kind in ("jumps", "normal"):
+        c = random_case(rng, cx, typ, order, it, ncomp=3, max_n=16, kind=kind)
+        op = cb.Op(typ, order, it)
+        u, v = c["crse"], rng.standard_normal((3,) + box_shape(c["flo"], c["fhi"]))
+        v *= region_mask(c["flo"], c["fhi"], c["rlo"], c["rhi"])
+        ptv = torch.full(u.shape, np.nan, dtype=torch.float64, device="cuda")
+        cb.prolong_adjoint_box(op, cuda(u), c["clo"], c["chi"], cuda(v), c["flo"], c["fhi"],
+                               c["rlo"], c["rhi"], 3, ptv, per_group=bool(pg))
+        pu = torch.zeros((3,) + box_shape(c["flo"], c["fhi"]), dtype=torch.float64, device="cuda")
+        cb.prolong_box(op, cuda(u), c["clo"], c["chi"], pu, c["flo"], c["fhi"], c["rlo"], c["rhi"],
+                       3, per_group=bool(pg))
+        torch.cuda.synchronize()
+        got = ptv.cpu().numpy()
+        want = np.zeros_like(u)
+        cx.prolong_adjoint(typ, order, it, pg, u, c["clo"], c["chi"], v, c["flo"], c["fhi"],
+                           c["rlo"], c["rhi"], 3, want)
+        scale = max(1.0, np.abs(want).max())
+        np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12 * scale,
+                                   err_msg=f"{typ} o{order} it{it} pg{pg} {kind}")
+        lhs = float(np.sum(pu.cpu().numpy() * v))
+        rhs = float(np.sum(u * got))
+        assert abs(lhs - rhs) <= 1e-12 * np.sum(np.abs(u * got)), (typ, order, it, pg, lhs, rhs)
+    assert cb.lib().cx_check_device() == cb.CX_OK
