@@ -190,7 +190,7 @@ struct cx_level_plan {
   BoxDesc *d_boxes = nullptr;
   TileRef *d_tiles = nullptr;
   int nsep_tiles = 0;
-  // items of z-window group g: [group_off[g], group_off[g + 1]) of d_tiles
+  // items of kernel group g: [group_off[g], group_off[g + 1]) of d_tiles
   int group_off[kStrGroups + 1] = {};
   int group_grid[kStrGroups] = {};
   int64_t nfine = 0, bytes = 0;
@@ -270,7 +270,7 @@ int cx_prolong_box_diag(cx_op_t op, const double *crse, const int crse_lo[3], co
     return e;
   cudaStream_t s = (cudaStream_t)stream;
   if (use_stream(op, per_group)) // one box per launch: spread it over the GPU
-    stream_tiling(b, stream_level_grid(stream_pair_of(b.kind[0], b.kind[1], b.kind[2])));
+    stream_tiling(b, stream_level_grid(stream_group_of(b.kind[0], b.kind[1], b.kind[2])));
   if (use_stream(op, per_group) && !shifts && !fallback)
     return cuda_status(launch_stream_box(b, s), "prolongation launch");
   if (use_stream(op, per_group)) {
@@ -356,7 +356,7 @@ int cx_level_plan_create(const cx_box_t *boxes, int nboxes, int per_group, cx_le
   // by z-window group (one kernel each), then by cost, largest first
   auto group_of = [&](const TileRef &t) {
     const BoxDesc &b = p->boxes[t.box];
-    return stream_pair_of(b.kind[0], b.kind[1], b.kind[2]);
+    return stream_group_of(b.kind[0], b.kind[1], b.kind[2]);
   };
   std::stable_sort(keyed.begin(), keyed.end(),
                    [&](const std::pair<int, TileRef> &a, const std::pair<int, TileRef> &b) {

@@ -51,16 +51,18 @@ struct TileRef {
 // Launchers (stream-ordered, no synchronisation).
 
 cudaError_t launch_stream_box(const BoxDesc &b, cudaStream_t s);
-// Streaming-kernel instantiation (stream_pairs.h) serving an operator's
-// kinds, -1 if none.
+// Stencil pair (stream_pairs.h) serving an operator's kinds, -1 if none.
 int stream_pair_of(int kx, int ky, int kz);
-constexpr int kStrGroups = 17; // number of instantiations (kStreamPairs)
+// Streaming-kernel instantiation serving an operator's kinds: 2 x pair + 1
+// if z is cell centred; -1 if none.
+int stream_group_of(int kx, int ky, int kz);
+constexpr int kStrGroups = 34; // number of instantiations (2 x kStreamPairs)
 // Level launch of the items of one instantiation; d_items holds only items
-// of boxes served by that pair.
-cudaError_t launch_stream_level(int pair, const BoxDesc *d_boxes,
+// of boxes served by that group.
+cudaError_t launch_stream_level(int group, const BoxDesc *d_boxes,
                                 const TileRef *d_items, int nitems, int grid,
                                 cudaStream_t s);
-int stream_level_grid(int pair);
+int stream_level_grid(int group);
 // Fills the streaming-kernel tiling of a box (tbase, ntile, zchunk, xcw,
 // npr, upi); min_items > 0 shortens the z chunks of a box launched alone so
 // that it spreads over at least that many CTAs where it can.

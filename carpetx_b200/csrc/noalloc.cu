@@ -115,7 +115,7 @@ extern "C" int cx_level_execute_noalloc(const cx_box_t *boxes, int nboxes, int p
       if (point[id])
         continue;
       const BoxDesc &b = g_stage.boxes[id];
-      const int g = stream_pair_of(b.kind[0], b.kind[1], b.kind[2]);
+      const int g = stream_group_of(b.kind[0], b.kind[1], b.kind[2]);
       for (int c = 0; c < b.ncomp; ++c)
         for (int tz = 0; tz < b.ntile[2]; ++tz)
           for (int tx = 0; tx < b.ntile[0]; ++tx) {

@@ -1,6 +1,8 @@
 // Separable prolongation, column-streaming kernel (all linear families and
 // minmod), templated on the operator's pair of 1-D stencil kinds: KV for its
-// vertex-centred directions, KC for its cell-centred ones.
+// vertex-centred directions, KC for its cell-centred ones, and on the
+// centring of z (CZ = 1: cell centred), so that the z ring holds exactly the
+// z kind's window and the z pass has a single stencil.
 //
 // A work item is one component of a block of up to NU fine "units" of a box
 // over a chunk of fine z; a unit is a column (fine x, pair of fine y sharing
@@ -29,6 +31,7 @@
 #pragma once
 #include "cx_internal.h"
 #include "cx_stencils.cuh"
+#include <type_traits>
 
 namespace cxb {
 namespace stream {
@@ -122,7 +125,7 @@ struct Item {
   int clo_z, nlo_z, nhi_z;
   int c_first, c_last; // coarse planes streamed
   int pxw;             // row pitch of the x-pass result
-  int ccx, ccy, ccz;   // 1: the direction is cell centred (KC), 0: vertex (KV)
+  int ccx, ccy;        // 1: the direction is cell centred (KC), 0: vertex (KV)
   // this thread's units (tid and tid + NTS of the block): y window start in
   // xs (-1: inactive unit); address of (fx, fy0) at fz = 0 (fy0 + 1 is fnx
   // further); colmask bit j: fy0 + j inside the region
@@ -153,16 +156,18 @@ __device__ __forceinline__ void load_plane(const Item &it, int c, double *S0) {
   }
 }
 
-template <class KV, class KC> struct PairInfo {
-  static constexpr int ZLO = KV::RLO < KC::RLO ? KV::RLO : KC::RLO;
-  static constexpr int ZHI = KV::RHI > KC::RHI ? KV::RHI : KC::RHI;
+// The z kind of an instantiation and its window [ZLO, ZHI] (coarse planes
+// relative to the centre).
+template <class KV, class KC, int CZ> struct ZKind {
+  using K = std::conditional_t<CZ != 0, KC, KV>;
+  static constexpr int ZLO = K::RLO, ZHI = K::RHI;
 };
 
-// Streams one item.  The ring covers the union of the two kinds' z windows
-// [ZLO, ZHI]; planes outside the z kind's read range are zero-filled and do
-// not reach its stencil.
-template <class KV, class KC> __device__ __forceinline__ void stream_item(Shared &sh, const Item &it) {
-  constexpr int ZLO = PairInfo<KV, KC>::ZLO, ZHI = PairInfo<KV, KC>::ZHI;
+// Streams one item.  The ring covers the z kind's window [ZLO, ZHI].
+template <class KV, class KC, int CZ>
+__device__ __forceinline__ void stream_item(Shared &sh, const Item &it) {
+  using KZ = typename ZKind<KV, KC, CZ>::K;
+  constexpr int ZLO = KZ::RLO, ZHI = KZ::RHI;
   constexpr int L = ZHI - ZLO + 1;
   double ring[L][UPT][FYT];
 #pragma unroll
@@ -228,11 +233,7 @@ template <class KV, class KC> __device__ __forceinline__ void stream_item(Shared
 #pragma unroll
             for (int i = 0; i < L; ++i)
               v[i] = ring[i][q][j];
-            double r;
-            if (it.ccz)
-              r = off ? KC::template ap<1>(v - ZLO) : KC::template ap<0>(v - ZLO);
-            else
-              r = off ? KV::template ap<1>(v - ZLO) : KV::template ap<0>(v - ZLO);
+            const double r = off ? KZ::template ap<1>(v - ZLO) : KZ::template ap<0>(v - ZLO);
             if (it.colmask[q] & (1 << j))
               __stcs(it.col[q] + j * it.fnx + (int64_t)fz * it.fplane, r);
           }
@@ -245,7 +246,7 @@ template <class KV, class KC> __device__ __forceinline__ void stream_item(Shared
 }
 
 // Geometry of work item (x chunk, unit block, z chunk, comp) of box b, for
-// the pair's streaming window [zwlo, zwhi] (union of the two z windows).
+// the z kind's streaming window [zwlo, zwhi].
 // The item's units are the unit block's consecutive (pair row, fine x)
 // columns of the x chunk, flattened x fastest; thread t owns unit t.
 // Returns false if the block holds no unit (box mode, narrow last chunk).
@@ -254,7 +255,6 @@ __device__ __forceinline__ bool make_item(const BoxDesc &b, int xchunk, int ublo
   const int kx = b.kind[0], ky = b.kind[1];
   it.ccx = kind_info(kx).cent;
   it.ccy = kind_info(ky).cent;
-  it.ccz = kind_info(b.kind[2]).cent;
   const int xb = b.tbase[0] + xchunk * b.xcw;
   const int W = min(b.xcw, b.rhi[0] - xb + 1);
   const int nunits = b.npr * W;
@@ -336,13 +336,14 @@ __device__ __forceinline__ bool make_item(const BoxDesc &b, int xchunk, int ublo
   return true;
 }
 
-template <class KV, class KC>
+template <class KV, class KC, int CZ>
 __device__ __forceinline__ void run_item(Shared &sh, const BoxDesc &b, int xchunk, int ublock,
                                          int zchunk, int comp) {
   Item it;
   // uniform over the CTA: an empty block is skipped by every thread
-  if (make_item(b, xchunk, ublock, zchunk, comp, PairInfo<KV, KC>::ZLO, PairInfo<KV, KC>::ZHI, it))
-    stream_item<KV, KC>(sh, it);
+  if (make_item(b, xchunk, ublock, zchunk, comp, ZKind<KV, KC, CZ>::ZLO, ZKind<KV, KC, CZ>::ZHI,
+                it))
+    stream_item<KV, KC, CZ>(sh, it);
 }
 
 constexpr int BOX_WORDS = (int)(sizeof(BoxDesc) / sizeof(int));
@@ -353,10 +354,10 @@ static_assert(BOX_WORDS <= NTS, "one thread per descriptor word");
 // list (sorted by cost, largest first) dealt round-robin to persistent CTAs;
 // the descriptors of the next item are loaded into registers while the
 // current item streams, so no global-memory latency sits between two items.
-// Two CTAs per SM (at most 128 registers), except the order-7 pairs whose
-// register ring (9 planes) needs more: one CTA per SM.
-template <class KV, class KC>
-__global__ void __launch_bounds__(NTS, PairInfo<KV, KC>::ZHI - PairInfo<KV, KC>::ZLO >= 8 ? 1 : 2)
+// Two CTAs per SM (at most 128 registers), except the order-7 z kinds whose
+// register ring (8 or 9 planes) needs more: one CTA per SM.
+template <class KV, class KC, int CZ>
+__global__ void __launch_bounds__(NTS, ZKind<KV, KC, CZ>::ZHI - ZKind<KV, KC, CZ>::ZLO >= 7 ? 1 : 2)
     stream_kernel(const BoxDesc b, const BoxDesc *__restrict__ boxes,
                   const TileRef *__restrict__ items, int nitems) {
   extern __shared__ __align__(16) unsigned char smem_raw[]; // sizeof(Shared) bytes
@@ -370,7 +371,7 @@ __global__ void __launch_bounds__(NTS, PairInfo<KV, KC>::ZHI - PairInfo<KV, KC>:
       r /= b.ntile[1];
       const int zchunk = r % b.ntile[2];
       const int comp = r / b.ntile[2];
-      run_item<KV, KC>(sh, b, xchunk, ublock, zchunk, comp);
+      run_item<KV, KC, CZ>(sh, b, xchunk, ublock, zchunk, comp);
     }
     return;
   }
@@ -397,7 +398,7 @@ __global__ void __launch_bounds__(NTS, PairInfo<KV, KC>::ZHI - PairInfo<KV, KC>:
       if (nxt + (int)gridDim.x < nitems)
         t_next2 = items[nxt + gridDim.x];
     }
-    run_item<KV, KC>(sh, box_s, t_cur.tx, t_cur.ty, t_cur.tz, t_cur.comp);
+    run_item<KV, KC, CZ>(sh, box_s, t_cur.tx, t_cur.ty, t_cur.tz, t_cur.comp);
     if (nxt >= nitems)
       break;
     cur = nxt;

@@ -4,33 +4,35 @@
 
 namespace cxb {
 namespace stream {
-KernelFn kernel_part0(int pair);
-KernelFn kernel_part1(int pair);
-KernelFn kernel_part2(int pair);
-KernelFn kernel_part3(int pair);
+KernelFn kernel_part0(int group);
+KernelFn kernel_part1(int group);
+KernelFn kernel_part2(int group);
+KernelFn kernel_part3(int group);
 
 namespace {
-bool g_attr_set[kStreamPairs] = {};
+bool g_attr_set[kStrGroups] = {};
 
-// Kernel of a pair; the first lookup allows its dynamic shared memory
+// Kernel of a group; the first lookup allows its dynamic shared memory
 // (sizeof(Shared), which may exceed the 48 KB default).
-KernelFn kernel_for(int pair) {
-  KernelFn k = kernel_part0(pair);
+KernelFn kernel_for(int group) {
+  if (group < 0 || group >= kStrGroups)
+    return nullptr;
+  KernelFn k = kernel_part0(group);
   if (!k)
-    k = kernel_part1(pair);
+    k = kernel_part1(group);
   if (!k)
-    k = kernel_part2(pair);
+    k = kernel_part2(group);
   if (!k)
-    k = kernel_part3(pair);
-  if (k && pair >= 0 && pair < kStreamPairs && !g_attr_set[pair]) {
+    k = kernel_part3(group);
+  if (k && !g_attr_set[group]) {
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Shared));
-    g_attr_set[pair] = true;
+    g_attr_set[group] = true;
   }
   return k;
 }
 
 int g_sms = 0;
-int g_grid[kStreamPairs] = {};
+int g_grid[kStrGroups] = {};
 
 int sms() {
   if (!g_sms) {
@@ -68,6 +70,11 @@ int stream_pair_of(int kx, int ky, int kz) {
   return -1;
 }
 
+int stream_group_of(int kx, int ky, int kz) {
+  const int pair = stream_pair_of(kx, ky, kz);
+  return pair < 0 ? -1 : 2 * pair + (kind_info(kz).cent == CC ? 1 : 0);
+}
+
 void stream_tiling(BoxDesc &b, int min_items) {
   using namespace stream;
   for (int d = 0; d < 3; ++d)
@@ -102,16 +109,17 @@ void stream_tiling(BoxDesc &b, int min_items) {
   b.ntile[2] = (E + zc - 1) / zc;
 }
 
-int stream_level_grid(int pair) {
+int stream_level_grid(int group) {
   using namespace stream;
-  if (pair < 0 || pair >= kStreamPairs)
+  KernelFn k = kernel_for(group);
+  if (!k)
     return 0;
-  if (!g_grid[pair]) {
+  if (!g_grid[group]) {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel_for(pair), NTS, sizeof(Shared));
-    g_grid[pair] = sms() * (per_sm > 0 ? per_sm : 1);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NTS, sizeof(Shared));
+    g_grid[group] = sms() * (per_sm > 0 ? per_sm : 1);
   }
-  return g_grid[pair];
+  return g_grid[group];
 }
 
 cudaError_t launch_stream_box(const BoxDesc &b, cudaStream_t s) {
@@ -121,22 +129,22 @@ cudaError_t launch_stream_box(const BoxDesc &b, cudaStream_t s) {
     return cudaSuccess;
   if (n64 > INT32_MAX)
     return cudaErrorInvalidValue;
-  const int pair = stream_pair_of(b.kind[0], b.kind[1], b.kind[2]);
-  KernelFn k = pair >= 0 ? kernel_for(pair) : nullptr;
+  const int group = stream_group_of(b.kind[0], b.kind[1], b.kind[2]);
+  KernelFn k = kernel_for(group);
   if (!k)
     return cudaErrorInvalidValue;
   const int n = (int)n64;
-  const int cap = stream_level_grid(pair);
+  const int cap = stream_level_grid(group);
   k<<<n < cap ? n : cap, NTS, sizeof(Shared), s>>>(b, nullptr, nullptr, n);
   return cudaGetLastError();
 }
 
-cudaError_t launch_stream_level(int pair, const BoxDesc *d_boxes, const TileRef *d_items,
+cudaError_t launch_stream_level(int group, const BoxDesc *d_boxes, const TileRef *d_items,
                                 int nitems, int grid, cudaStream_t s) {
   using namespace stream;
   if (nitems <= 0)
     return cudaSuccess;
-  KernelFn k = kernel_for(pair);
+  KernelFn k = kernel_for(group);
   if (!k)
     return cudaErrorInvalidValue;
   BoxDesc unused{};

@@ -1,18 +1,22 @@
-// Streaming-kernel instantiations, part 1 of kStreamParts (the pairs of
-// stream_pairs.h whose index is 1 modulo kStreamParts; split only to compile
-// in parallel).
+// Streaming-kernel instantiations, part 1 of kStreamParts: the kernels whose
+// group (2 x pair index of stream_pairs.h + 1 for a cell-centred z) is 1
+// modulo kStreamParts; split only to compile in parallel.
 #include "stream_kernel.cuh"
 #include "stream_pairs.h"
 
 namespace cxb {
 namespace stream {
 
-KernelFn kernel_part1(int pair) {
-  switch (pair) {
+KernelFn kernel_part1(int group) {
+  switch (group) {
 #define CXB_PAIR_CASE(I, V, C, KVI, KCI)                                       \
-  case I:                                                                      \
-    if constexpr (I % kStreamParts == 1)                                      \
-      return stream_kernel<V, C>;                                              \
+  case 2 * I:                                                                  \
+    if constexpr ((2 * I) % kStreamParts == 1)                                \
+      return stream_kernel<V, C, 0>;                                           \
+    break;                                                                     \
+  case 2 * I + 1:                                                              \
+    if constexpr ((2 * I + 1) % kStreamParts == 1)                            \
+      return stream_kernel<V, C, 1>;                                           \
     break;
     CXB_STREAM_PAIRS(CXB_PAIR_CASE)
 #undef CXB_PAIR_CASE
