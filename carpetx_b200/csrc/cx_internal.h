@@ -53,10 +53,11 @@ struct TileRef {
 cudaError_t launch_stream_box(const BoxDesc &b, cudaStream_t s);
 // Stencil pair (stream_pairs.h) serving an operator's kinds, -1 if none.
 int stream_pair_of(int kx, int ky, int kz);
-// Streaming-kernel instantiation serving an operator's kinds: 2 x pair + 1
-// if z is cell centred; -1 if none.
+// Streaming-kernel instantiation serving an operator's kinds:
+// 8 x pair + (cx << 2 | cy << 1 | cz), c = 1 for a cell-centred direction;
+// -1 if none.
 int stream_group_of(int kx, int ky, int kz);
-constexpr int kStrGroups = 34; // number of instantiations (2 x kStreamPairs)
+constexpr int kStrGroups = 136; // number of instantiations (8 x kStreamPairs)
 // Level launch of the items of one instantiation; d_items holds only items
 // of boxes served by that group.
 cudaError_t launch_stream_level(int group, const BoxDesc *d_boxes,

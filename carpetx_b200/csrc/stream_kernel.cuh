@@ -1,8 +1,9 @@
 // Separable prolongation, column-streaming kernel (all linear families and
 // minmod), templated on the operator's pair of 1-D stencil kinds: KV for its
 // vertex-centred directions, KC for its cell-centred ones, and on the
-// centring of z (CZ = 1: cell centred), so that the z ring holds exactly the
-// z kind's window and the z pass has a single stencil.
+// operator's centring CM = (cx << 2) | (cy << 1) | cz (1: cell centred), so
+// every pass has a single stencil and the z ring holds exactly the z kind's
+// window.
 //
 // A work item is one component of a block of up to NU fine "units" of a box
 // over a chunk of fine z; a unit is a column (fine x, pair of fine y sharing
@@ -125,7 +126,6 @@ struct Item {
   int clo_z, nlo_z, nhi_z;
   int c_first, c_last; // coarse planes streamed
   int pxw;             // row pitch of the x-pass result
-  int ccx, ccy;        // 1: the direction is cell centred (KC), 0: vertex (KV)
   // this thread's units (tid and tid + NTS of the block): y window start in
   // xs (-1: inactive unit); address of (fx, fy0) at fz = 0 (fy0 + 1 is fnx
   // further); colmask bit j: fy0 + j inside the region
@@ -156,17 +156,21 @@ __device__ __forceinline__ void load_plane(const Item &it, int c, double *S0) {
   }
 }
 
-// The z kind of an instantiation and its window [ZLO, ZHI] (coarse planes
-// relative to the centre).
-template <class KV, class KC, int CZ> struct ZKind {
-  using K = std::conditional_t<CZ != 0, KC, KV>;
-  static constexpr int ZLO = K::RLO, ZHI = K::RHI;
+// The stencil kinds of an instantiation per direction; [ZLO, ZHI] is the z
+// kind's window (coarse planes relative to the centre).
+template <class KV, class KC, int CM> struct Kinds {
+  using KX = std::conditional_t<(CM & 4) != 0, KC, KV>;
+  using KY = std::conditional_t<(CM & 2) != 0, KC, KV>;
+  using KZ = std::conditional_t<(CM & 1) != 0, KC, KV>;
+  static constexpr int ZLO = KZ::RLO, ZHI = KZ::RHI;
 };
 
 // Streams one item.  The ring covers the z kind's window [ZLO, ZHI].
-template <class KV, class KC, int CZ>
+template <class KV, class KC, int CM>
 __device__ __forceinline__ void stream_item(Shared &sh, const Item &it) {
-  using KZ = typename ZKind<KV, KC, CZ>::K;
+  using KX = typename Kinds<KV, KC, CM>::KX;
+  using KY = typename Kinds<KV, KC, CM>::KY;
+  using KZ = typename Kinds<KV, KC, CM>::KZ;
   constexpr int ZLO = KZ::RLO, ZHI = KZ::RHI;
   constexpr int L = ZHI - ZLO + 1;
   double ring[L][UPT][FYT];
@@ -192,10 +196,7 @@ __device__ __forceinline__ void stream_item(Shared &sh, const Item &it) {
     for (int k = 0; k < XTMAX; ++k) {
       if (it.xt_src[k] < 0)
         continue;
-      if (it.ccx)
-        xtask<KC>(sh.s0[slot] + it.xt_src[k], sh.xs + it.xt_dst[k]);
-      else
-        xtask<KV>(sh.s0[slot] + it.xt_src[k], sh.xs + it.xt_dst[k]);
+      xtask<KX>(sh.s0[slot] + it.xt_src[k], sh.xs + it.xt_dst[k]);
     }
     __syncthreads();
 #pragma unroll
@@ -208,12 +209,8 @@ __device__ __forceinline__ void stream_item(Shared &sh, const Item &it) {
 #pragma unroll
     for (int q = 0; q < UPT; ++q) {
       double y[FYT] = {0.0, 0.0};
-      if (it.ysrc[q] >= 0) {
-        if (it.ccy)
-          ypass<KC>(sh.xs + it.ysrc[q], it.pxw, y);
-        else
-          ypass<KV>(sh.xs + it.ysrc[q], it.pxw, y);
-      }
+      if (it.ysrc[q] >= 0)
+        ypass<KY>(sh.xs + it.ysrc[q], it.pxw, y);
 #pragma unroll
       for (int j = 0; j < FYT; ++j)
         ring[L - 1][q][j] = y[j];
@@ -253,8 +250,6 @@ __device__ __forceinline__ void stream_item(Shared &sh, const Item &it) {
 __device__ __forceinline__ bool make_item(const BoxDesc &b, int xchunk, int ublock, int zchunk,
                                           int comp, int zwlo, int zwhi, Item &it) {
   const int kx = b.kind[0], ky = b.kind[1];
-  it.ccx = kind_info(kx).cent;
-  it.ccy = kind_info(ky).cent;
   const int xb = b.tbase[0] + xchunk * b.xcw;
   const int W = min(b.xcw, b.rhi[0] - xb + 1);
   const int nunits = b.npr * W;
@@ -336,14 +331,14 @@ __device__ __forceinline__ bool make_item(const BoxDesc &b, int xchunk, int ublo
   return true;
 }
 
-template <class KV, class KC, int CZ>
+template <class KV, class KC, int CM>
 __device__ __forceinline__ void run_item(Shared &sh, const BoxDesc &b, int xchunk, int ublock,
                                          int zchunk, int comp) {
   Item it;
   // uniform over the CTA: an empty block is skipped by every thread
-  if (make_item(b, xchunk, ublock, zchunk, comp, ZKind<KV, KC, CZ>::ZLO, ZKind<KV, KC, CZ>::ZHI,
+  if (make_item(b, xchunk, ublock, zchunk, comp, Kinds<KV, KC, CM>::ZLO, Kinds<KV, KC, CM>::ZHI,
                 it))
-    stream_item<KV, KC, CZ>(sh, it);
+    stream_item<KV, KC, CM>(sh, it);
 }
 
 constexpr int BOX_WORDS = (int)(sizeof(BoxDesc) / sizeof(int));
@@ -356,8 +351,8 @@ static_assert(BOX_WORDS <= NTS, "one thread per descriptor word");
 // current item streams, so no global-memory latency sits between two items.
 // Two CTAs per SM (at most 128 registers), except the order-7 z kinds whose
 // register ring (8 or 9 planes) needs more: one CTA per SM.
-template <class KV, class KC, int CZ>
-__global__ void __launch_bounds__(NTS, ZKind<KV, KC, CZ>::ZHI - ZKind<KV, KC, CZ>::ZLO >= 7 ? 1 : 2)
+template <class KV, class KC, int CM>
+__global__ void __launch_bounds__(NTS, Kinds<KV, KC, CM>::ZHI - Kinds<KV, KC, CM>::ZLO >= 7 ? 1 : 2)
     stream_kernel(const BoxDesc b, const BoxDesc *__restrict__ boxes,
                   const TileRef *__restrict__ items, int nitems) {
   extern __shared__ __align__(16) unsigned char smem_raw[]; // sizeof(Shared) bytes
@@ -371,7 +366,7 @@ __global__ void __launch_bounds__(NTS, ZKind<KV, KC, CZ>::ZHI - ZKind<KV, KC, CZ
       r /= b.ntile[1];
       const int zchunk = r % b.ntile[2];
       const int comp = r / b.ntile[2];
-      run_item<KV, KC, CZ>(sh, b, xchunk, ublock, zchunk, comp);
+      run_item<KV, KC, CM>(sh, b, xchunk, ublock, zchunk, comp);
     }
     return;
   }
@@ -398,7 +393,7 @@ __global__ void __launch_bounds__(NTS, ZKind<KV, KC, CZ>::ZHI - ZKind<KV, KC, CZ
       if (nxt + (int)gridDim.x < nitems)
         t_next2 = items[nxt + gridDim.x];
     }
-    run_item<KV, KC, CZ>(sh, box_s, t_cur.tx, t_cur.ty, t_cur.tz, t_cur.comp);
+    run_item<KV, KC, CM>(sh, box_s, t_cur.tx, t_cur.ty, t_cur.tz, t_cur.comp);
     if (nxt >= nitems)
       break;
     cur = nxt;

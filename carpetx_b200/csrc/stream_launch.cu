@@ -8,6 +8,10 @@ KernelFn kernel_part0(int group);
 KernelFn kernel_part1(int group);
 KernelFn kernel_part2(int group);
 KernelFn kernel_part3(int group);
+KernelFn kernel_part4(int group);
+KernelFn kernel_part5(int group);
+KernelFn kernel_part6(int group);
+KernelFn kernel_part7(int group);
 
 namespace {
 bool g_attr_set[kStrGroups] = {};
@@ -17,13 +21,10 @@ bool g_attr_set[kStrGroups] = {};
 KernelFn kernel_for(int group) {
   if (group < 0 || group >= kStrGroups)
     return nullptr;
-  KernelFn k = kernel_part0(group);
-  if (!k)
-    k = kernel_part1(group);
-  if (!k)
-    k = kernel_part2(group);
-  if (!k)
-    k = kernel_part3(group);
+  static KernelFn (*const parts[kStreamParts])(int) = {kernel_part0, kernel_part1, kernel_part2,
+                                                        kernel_part3, kernel_part4, kernel_part5,
+                                                        kernel_part6, kernel_part7};
+  KernelFn k = parts[group % kStreamParts](group);
   if (k && !g_attr_set[group]) {
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Shared));
     g_attr_set[group] = true;
@@ -72,7 +73,9 @@ int stream_pair_of(int kx, int ky, int kz) {
 
 int stream_group_of(int kx, int ky, int kz) {
   const int pair = stream_pair_of(kx, ky, kz);
-  return pair < 0 ? -1 : 2 * pair + (kind_info(kz).cent == CC ? 1 : 0);
+  const int cm = (kind_info(kx).cent == CC ? 4 : 0) | (kind_info(ky).cent == CC ? 2 : 0) |
+                 (kind_info(kz).cent == CC ? 1 : 0);
+  return pair < 0 ? -1 : kStreamParts * pair + cm;
 }
 
 void stream_tiling(BoxDesc &b, int min_items) {

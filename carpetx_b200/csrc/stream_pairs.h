@@ -28,5 +28,5 @@
 
 namespace cxb {
 constexpr int kStreamPairs = 17;
-constexpr int kStreamParts = 4; // instantiations are spread over 4 files
+constexpr int kStreamParts = 8; // one file per centring (8 instantiations per pair)
 } // namespace cxb

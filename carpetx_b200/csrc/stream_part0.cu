@@ -1,6 +1,6 @@
 // Streaming-kernel instantiations, part 0 of kStreamParts: the kernels whose
-// group (2 x pair index of stream_pairs.h + 1 for a cell-centred z) is 0
-// modulo kStreamParts; split only to compile in parallel.
+// centring (cx << 2 | cy << 1 | cz) is 0, one per stencil pair of
+// stream_pairs.h; split only to compile in parallel.
 #include "stream_kernel.cuh"
 #include "stream_pairs.h"
 
@@ -10,14 +10,8 @@ namespace stream {
 KernelFn kernel_part0(int group) {
   switch (group) {
 #define CXB_PAIR_CASE(I, V, C, KVI, KCI)                                       \
-  case 2 * I:                                                                  \
-    if constexpr ((2 * I) % kStreamParts == 0)                                \
-      return stream_kernel<V, C, 0>;                                           \
-    break;                                                                     \
-  case 2 * I + 1:                                                              \
-    if constexpr ((2 * I + 1) % kStreamParts == 0)                            \
-      return stream_kernel<V, C, 1>;                                           \
-    break;
+  case kStreamParts * I + 0:                                                   \
+    return stream_kernel<V, C, 0>;
     CXB_STREAM_PAIRS(CXB_PAIR_CASE)
 #undef CXB_PAIR_CASE
   default:
