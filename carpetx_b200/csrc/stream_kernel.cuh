@@ -21,6 +21,8 @@
 //   z pass  each thread keeps the Y values of the last L coarse planes in a
 //           register ring; once the ring holds the stencil of coarse centre
 //           cc it emits fine z = 2cc and 2cc+1 straight to global memory.
+//           The plane loop is unrolled by L, so the ring rotates by register
+//           renaming instead of moving L - 1 entries per plane.
 // Every coarse value is read from HBM once per column (plus the column's x/y
 // halo, which the L2 serves), every intermediate stays on chip, and the fine
 // data is written once with coalesced streaming stores.  The arithmetic of
@@ -136,12 +138,16 @@ struct Item {
   int64_t fplane;
   int zlo, zhi; // fine z emitted (inclusive)
   // coarse plane loads: smem offset (-1: none) and offset within the coarse
-  // z plane (-1: outside the read range in x or y, zero-filled)
+  // z plane (-1: outside the read range in x or y, zero-filled); rounds of
+  // NTS loads the item needs (the same for every thread)
   int ld_soff[LDMAX];
   int ld_goff[LDMAX];
-  // x-pass tasks: smem offsets into the plane and into xs (-1: none)
+  int nld;
+  // x-pass tasks: smem offsets into the plane and into xs (-1: none); rounds
+  // of NTS tasks the item needs
   int xt_src[XTMAX];
   int xt_dst[XTMAX];
+  int nxt;
 };
 
 __device__ __forceinline__ void load_plane(const Item &it, int c, double *S0) {
@@ -149,6 +155,8 @@ __device__ __forceinline__ void load_plane(const Item &it, int c, double *S0) {
   const double *pb = it.cbase + (int64_t)(c - it.clo_z) * it.cplane;
 #pragma unroll
   for (int i = 0; i < LDMAX; ++i) {
+    if (i >= it.nld)
+      break;
     if (it.ld_soff[i] < 0)
       continue;
     const bool ok = zok && it.ld_goff[i] >= 0;
@@ -181,63 +189,66 @@ __device__ __forceinline__ void stream_item(Shared &sh, const Item &it) {
     cp_async_commit();
   }
   int slot = 0;
-  for (int c = it.c_first; c <= it.c_last; ++c) {
-    {
-      int ls = slot + DPF;
-      if (ls >= NRING)
-        ls -= NRING;
-      if (c + DPF <= it.c_last)
-        load_plane(it, c + DPF, sh.s0[ls]);
-      cp_async_commit();
-    }
-    cp_async_wait_dpf();
-    __syncthreads();
+  for (int c0 = it.c_first; c0 <= it.c_last; c0 += L) {
 #pragma unroll
-    for (int k = 0; k < XTMAX; ++k) {
-      if (it.xt_src[k] < 0)
-        continue;
-      xtask<KX>(sh.s0[slot] + it.xt_src[k], sh.xs + it.xt_dst[k]);
-    }
-    __syncthreads();
+    for (int ph = 0; ph < L; ++ph) {
+      const int c = c0 + ph;
+      if (c > it.c_last)
+        break;
+      {
+        int ls = slot + DPF;
+        if (ls >= NRING)
+          ls -= NRING;
+        if (c + DPF <= it.c_last)
+          load_plane(it, c + DPF, sh.s0[ls]);
+        cp_async_commit();
+      }
+      cp_async_wait_dpf();
+      __syncthreads();
 #pragma unroll
-    for (int i = 0; i < L - 1; ++i)
+      for (int k = 0; k < XTMAX; ++k) {
+        if (k >= it.nxt)
+          break;
+        if (it.xt_src[k] < 0)
+          continue;
+        xtask<KX>(sh.s0[slot] + it.xt_src[k], sh.xs + it.xt_dst[k]);
+      }
+      __syncthreads();
+      // ring slot ph takes plane c; logical position i (0 oldest) is slot
+      // (ph + 1 + i) % L
 #pragma unroll
-      for (int q = 0; q < UPT; ++q)
+      for (int q = 0; q < UPT; ++q) {
+        double y[FYT] = {0.0, 0.0};
+        if (it.ysrc[q] >= 0)
+          ypass<KY>(sh.xs + it.ysrc[q], it.pxw, y);
 #pragma unroll
         for (int j = 0; j < FYT; ++j)
-          ring[i][q][j] = ring[i + 1][q][j];
-#pragma unroll
-    for (int q = 0; q < UPT; ++q) {
-      double y[FYT] = {0.0, 0.0};
-      if (it.ysrc[q] >= 0)
-        ypass<KY>(sh.xs + it.ysrc[q], it.pxw, y);
-#pragma unroll
-      for (int j = 0; j < FYT; ++j)
-        ring[L - 1][q][j] = y[j];
-    }
-    if (c - it.c_first >= L - 1) {
-      const int cc = c - ZHI; // coarse centre whose stencil is complete
-#pragma unroll
-      for (int off = 0; off < 2; ++off) {
-        const int fz = 2 * cc + off;
-        if (fz < it.zlo || fz > it.zhi)
-          continue;
-#pragma unroll
-        for (int q = 0; q < UPT; ++q)
-#pragma unroll
-          for (int j = 0; j < FYT; ++j) {
-            double v[L];
-#pragma unroll
-            for (int i = 0; i < L; ++i)
-              v[i] = ring[i][q][j];
-            const double r = off ? KZ::template ap<1>(v - ZLO) : KZ::template ap<0>(v - ZLO);
-            if (it.colmask[q] & (1 << j))
-              __stcs(it.col[q] + j * it.fnx + (int64_t)fz * it.fplane, r);
-          }
+          ring[ph][q][j] = y[j];
       }
+      if (c - it.c_first >= L - 1) {
+        const int cc = c - ZHI; // coarse centre whose stencil is complete
+#pragma unroll
+        for (int off = 0; off < 2; ++off) {
+          const int fz = 2 * cc + off;
+          if (fz < it.zlo || fz > it.zhi)
+            continue;
+#pragma unroll
+          for (int q = 0; q < UPT; ++q)
+#pragma unroll
+            for (int j = 0; j < FYT; ++j) {
+              double v[L];
+#pragma unroll
+              for (int i = 0; i < L; ++i)
+                v[i] = ring[(ph + 1 + i) % L][q][j];
+              const double r = off ? KZ::template ap<1>(v - ZLO) : KZ::template ap<0>(v - ZLO);
+              if (it.colmask[q] & (1 << j))
+                __stcs(it.col[q] + j * it.fnx + (int64_t)fz * it.fplane, r);
+            }
+        }
+      }
+      if (++slot == NRING)
+        slot = 0;
     }
-    if (++slot == NRING)
-      slot = 0;
   }
   __syncthreads(); // the next item reuses the plane ring and xs
 }
@@ -302,6 +313,7 @@ __device__ __forceinline__ bool make_item(const BoxDesc &b, int xchunk, int ublo
   }
   // coarse plane window: NR rows x Wx columns
   const int n = NR * Wx;
+  it.nld = (n + NTS - 1) / NTS;
 #pragma unroll
   for (int i = 0; i < LDMAX; ++i) {
     const int e = threadIdx.x + i * NTS;
@@ -317,6 +329,7 @@ __device__ __forceinline__ bool make_item(const BoxDesc &b, int xchunk, int ublo
   }
   // x-pass tasks: NR rows x nseg segments, rows fastest
   const int nt = NR * nseg;
+  it.nxt = (nt + NTS - 1) / NTS;
 #pragma unroll
   for (int k = 0; k < XTMAX; ++k) {
     const int t = threadIdx.x + k * NTS;

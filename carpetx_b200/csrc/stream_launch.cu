@@ -97,12 +97,13 @@ void stream_tiling(BoxDesc &b, int min_items) {
   b.npr = (b.rhi[1] - b.tbase[1]) / 2 + 1;
   b.upi = NU < PRMAX * b.xcw ? NU : PRMAX * b.xcw;
   b.ntile[1] = (b.npr * b.xcw + b.upi - 1) / b.upi;
-  // fine z per item: whole columns up to 96 fine points, else near-equal
-  // even chunks of at most 96 (the z halo costs extra planes per chunk);
-  // shorter chunks (down to 16) when the box alone must fill min_items CTAs
+  // fine z per item: whole columns up to 128 fine points, else near-equal
+  // even chunks of at most 128 (the z halo and the pipeline start cost extra
+  // planes per chunk); shorter chunks (down to 16) when the box alone must
+  // fill min_items CTAs
   const int E = b.rhi[2] - b.tbase[2] + 1;
   const int64_t xy_items = (int64_t)b.ntile[0] * b.ntile[1] * b.ncomp;
-  int maxz = 96;
+  int maxz = 128;
   while (maxz > 16 && xy_items * ((E + maxz - 1) / maxz) < min_items)
     maxz /= 2;
   const int nch = (E + maxz - 1) / maxz;

@@ -161,7 +161,7 @@ int cx_level_plan_create_adjoint(const cx_box_t *boxes, int nboxes,
 
 /* Upper limits of cx_level_execute_noalloc: boxes per call, work items per
  * call (an item is one component of up to 512 fine columns of a box over a
- * chunk of at most 96 fine z points). */
+ * chunk of at most 128 fine z points). */
 #define CX_NOALLOC_MAX_BOXES 1024
 #define CX_NOALLOC_MAX_ITEMS 131072
 
