@@ -1,504 +1,22 @@
-// Transpose of the separable linear prolongations, streaming gather form (no
-// atomics), for one box per launch or a whole level per persistent launch.
-//
-// P = Pz Py Px (the x pass first) with 1-D maps P_d, so P^T = Px^T Py^T Pz^T
-// and the three 1-D transposes can be applied in any order.  In 1-D, fine
-// point f = 2 cc + off reads coarse cc + o with weight w(off, o), o in the
-// stencil of off; so coarse point c gathers
-//   crse_bar(c) = sum_{off, o} w(off, o) fine_bar(2 (c - o) + off).
-// With the fine window of c starting at 2 (c - RHI), tap m = 2 (RHI - o) + off
-// (0 <= m <= 2 (RHI - RLO) + 1) of that window has weight w(m & 1, RHI - m/2).
-//
-// A work item is a tile of up to NU coarse (x, y) columns of the coarse box
-// over a chunk of coarse z, one component.  The CTA streams the fine z planes
-// that reach the chunk through a ring of shared-memory buffers holding the
-// tile's fine footprint (its region points; the rest of the footprint reads
-// as zero):
-//   load   fine plane fz + DPF: one thread per footprint row issues one bulk
-//          (TMA) copy of the row's 16-byte aligned middle, completing on the
-//          buffer's mbarrier (each row is placed in shared memory with the
-//          parity of its global address, so both ends of the copy are 16-byte
-//          aligned); the odd first/last point of a row takes an 8-byte copy.
-//          The rows are dealt across the warps: a warp's bulk copies are
-//          issued one lane after the other, so spreading them shortens the
-//          issue;
-//   x^T    G(cx, fy) for the tile's coarse x and every footprint row, XB
-//          coarse x per task from a register window of the fine row, into
-//          shared memory (column major: the y taps of a column are adjacent);
-//   y^T    each thread gathers g(cx, cy) of its UPT columns;
-//   z^T    each thread accumulates w(off, o) g into the coarse planes
-//          cc + o that fine plane fz = 2 cc + off reaches (a register ring of
-//          L = RHI - RLO + 1 partial sums); when cc moves on, coarse plane
-//          cc + RLO is complete and is stored.
-// Every coarse point of the coarse box is written once (zero where no region
-// point reads it); sums run in a fixed order, so results are deterministic.
-// Fine data is read from HBM once; the footprint halo of a tile is read again
-// by its neighbours, from the L2 (tiles of a box are dealt together).
-#include <type_traits>
-
-#include "cx_internal.h"
-#include "cx_stencils.cuh"
-#include "cx_async.cuh"
-#include "stream_pairs.h"
+// Host side of the adjoint of the separable linear prolongations: kernel
+// lookup per stencil pair and centring, tiling, launches.  The kernel is in
+// adjoint_kernel.cuh; its instantiations are spread over adjoint_part*.cu.
+#include "adjoint_kernel.cuh"
 
 namespace cxb {
+using namespace adj;
 namespace {
 
-// 1-D weight of coarse offset o for a fine point with offset off: the
-// coefficient multiplying v[o] in the kind's linear form (0 outside its
-// stencil).  Same stencils as cx_stencils.cuh (impl.hxx:396-878).
-template <class K> struct Weight;
+constexpr int kAdjGroups = kStreamParts * kStreamPairs; // pair x centring
 
-template <int P> struct Weight<VcPoly<P>> {
-  CXB_HD static constexpr double w(int off, int o) {
-    if (off == 0)
-      return o == 0 ? 1.0 : 0.0;
-    constexpr int i0 = (P + 1) / 2 - 1;
-    if (o < -i0 || o > P - i0)
-      return 0.0;
-    return vc_poly_c<P>(o + i0); // symmetric pairs share c(i) = c(P - i)
-  }
-};
-template <int P> struct Weight<CcPoly<P>> {
-  CXB_HD static constexpr double w(int off, int o) {
-    constexpr int I0 = (P + 1) / 2;
-    if (off == 0) {
-      const int i = o + I0;
-      return i >= 0 && i <= P ? cc_poly_c<P>(i) : 0.0;
-    }
-    const int i = o + I0 - P % 2;
-    return i >= 0 && i <= P ? cc_poly_c<P>(P - i) : 0.0;
-  }
-};
-template <int P> struct Weight<CcCons<P>> {
-  CXB_HD static constexpr double w(int off, int o) {
-    constexpr int I0 = (P + 1) / 2;
-    if constexpr (P % 2 == 0) {
-      if (o == 0)
-        return cc_cons_c<P>(P / 2);
-      if (o < -P / 2 || o > P / 2)
-        return 0.0;
-      const double c = o < 0 ? cc_cons_c<P>(o + I0) : cc_cons_c<P>(P - o - I0);
-      return (o < 0) == (off == 0) ? c : -c;
-    } else {
-      if (off == 0) {
-        const int i = o + I0;
-        return i >= 0 && i <= P ? cc_cons_c<P>(i) : 0.0;
-      }
-      const int i = (P + 1) / 2 - o;
-      return i >= 0 && i <= P ? cc_cons_c<P>(i) : 0.0;
-    }
-  }
-};
-template <int P> struct Weight<VcCons<P>> {
-  CXB_HD static constexpr double w(int off, int o) {
-    if (off == 0)
-      return o == 0 ? 1.0 : 0.0;
-    if (P == 0)
-      return 0.0;
-    return o == 0 || o == 1 ? 0.5 : 0.0;
-  }
-};
-
-// weight of tap m of a coarse point's fine window
-template <class K> CXB_HD constexpr double wtap(int m) {
-  return Weight<K>::w(m & 1, K::RHI - (m >> 1));
-}
-template <class K> constexpr int DK = K::RHI - K::RLO;
-
-// A CTA of NT threads streams a tile of up to NT x UPT coarse columns (at
-// most TMAX per direction), two planes ahead; two CTAs per SM where the
-// shared memory allows (all but the order-7 pairs).  Measured on the
-// differentiated level (64 boxes of 32-96 coarse points per direction), this
-// beats one CTA of 512 threads with larger tiles (less footprint halo) and
-// one plane ahead: the time goes into waiting for the copies, and more CTAs
-// and planes in flight hide more of it.
-constexpr int NT = 256;       // threads per CTA
-constexpr int TMAX = 64;      // tile extent in x or y at most
-constexpr int DPF = 2;        // fine planes prefetched ahead
-constexpr int NBUF = DPF + 1; // shared fine-plane ring
-constexpr int XB = 4;         // coarse x per x^T task
-
-// Footprint of a TX x TY tile for stencil spread D <= DM: rows, row pitch
-// (odd, one more than the widest footprint row: a row is placed at offset 0
-// or 1 to match its global address parity), x^T column pitch (odd).
-CXB_HD constexpr int fp_rows(int ty, int dm) { return 2 * ty + 2 * dm; }
-CXB_HD constexpr int fp_pitch(int tx, int dm) { return 2 * tx + 2 * dm + 1; }
-CXB_HD constexpr int g_pitch(int ty, int dm) { return fp_rows(ty, dm) | 1; }
-CXB_HD constexpr int tile_ty(int tx, int nu) { return nu / tx < TMAX ? nu / tx : TMAX; }
-CXB_HD constexpr int max_fp(int dm, int nu, int what) {
-  int m = 0;
-  for (int tx = 1; tx <= TMAX; ++tx) {
-    const int ty = tile_ty(tx, nu);
-    const int nseg = (tx + XB - 1) / XB;
-    const int v = what == 0   ? fp_rows(ty, dm) * fp_pitch(tx, dm)
-                  : what == 1 ? tx * g_pitch(ty, dm)
-                              : nseg * fp_rows(ty, dm);
-    m = v > m ? v : m;
-  }
-  return m;
-}
-// coarse columns per thread
-CXB_HD constexpr int upt_of(int) { return 2; }
-
-template <class KV, class KC> struct AdjPair {
-  static constexpr int DM = DK<KV> > DK<KC> ? DK<KV> : DK<KC>;
-  static constexpr int UPT = upt_of(DM);
-  static constexpr int NU = NT * UPT; // coarse columns per item at most
-  static constexpr int FP = (max_fp(DM, NU, 0) + 1) & ~1; // fine footprint plane (even: 16-byte buffers)
-  static constexpr int GP = max_fp(DM, NU, 1);            // x^T result
-  static constexpr int XTMAX = (max_fp(DM, NU, 2) + NT - 1) / NT; // x^T tasks per thread
-  // the last x^T window of a row may run 2 (XB - 1) points past the row
-  static constexpr size_t SMEM = sizeof(double) * (size_t)(NBUF * FP + GP + 2 * XB);
-  static_assert(SMEM + 1024 <= 227 * 1024, "shared memory per CTA");
-  static constexpr int OCC = SMEM + 2048 <= 113 * 1024 ? 2 : 1; // CTAs per SM
-  static_assert(XTMAX <= 3, "x^T task registers");
-};
-
-__device__ __forceinline__ void cp_async8(double *sdst, const double *gsrc) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_dpf() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(DPF) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// Set when a bounded wait gave up (read and cleared by cx_check_device).
-__device__ int g_adj_timeout = 0;
-
-// x^T task: XB coarse x of one footprint row from a register window; only
-// the first n are stored (the window of the last task of a row may run past
-// the row: those points reach only unstored results).
-template <class K>
-__device__ __forceinline__ void xt_task(const double *__restrict__ src, double *__restrict__ dst,
-                                        int gpw, int n) {
-  constexpr int D = DK<K>, WIN = 2 * XB + 2 * D;
-  double v[WIN];
-#pragma unroll
-  for (int i = 0; i < WIN; ++i)
-    v[i] = src[i];
-#pragma unroll
-  for (int t = 0; t < XB; ++t) {
-    double acc = 0.0;
-#pragma unroll
-    for (int m = 0; m <= 2 * D + 1; ++m) {
-      const double w = wtap<K>(m);
-      if (w != 0.0)
-        acc = fma(w, v[2 * t + m], acc);
-    }
-    if (t < n)
-      dst[t * gpw] = acc;
-  }
-}
-
-// y^T of one column: the 2 D + 2 taps are adjacent in the x^T result.
-template <class K> __device__ __forceinline__ double yt_col(const double *__restrict__ src) {
-  constexpr int D = DK<K>;
-  double acc = 0.0;
-#pragma unroll
-  for (int m = 0; m <= 2 * D + 1; ++m) {
-    const double w = wtap<K>(m);
-    if (w != 0.0)
-      acc = fma(w, src[m], acc);
-  }
-  return acc;
-}
-
-// z^T: fine plane with offset OFF adds w(OFF, RLO + k) g to partial sum k.
-template <class K, int OFF, int L>
-__device__ __forceinline__ void zt_add(double (&acc)[L], double g) {
-#pragma unroll
-  for (int k = 0; k < L; ++k) {
-    const double w = Weight<K>::w(OFF, K::RLO + k);
-    if (w != 0.0)
-      acc[k] = fma(w, g, acc[k]);
-  }
-}
-
-// One item: coarse tile (xt, yt), coarse z chunk zt, component comp of box b.
-// Returns false if a bounded wait gave up (the CTA then stops).
-template <class KV, class KC, class KZ>
-__device__ __forceinline__ bool adj_item(double *fbuf, double *gbuf, uint64_t *mbar, int *s_fail,
-                                         uint32_t &phase, const BoxDesc &bd, int xt, int yt, int zt,
-                                         int comp) {
-  constexpr int FP = AdjPair<KV, KC>::FP, DM = AdjPair<KV, KC>::DM;
-  constexpr int UPT = AdjPair<KV, KC>::UPT, XTMAX = AdjPair<KV, KC>::XTMAX;
-  constexpr int L = DK<KZ> + 1;
-  const int tid = threadIdx.x;
-  // the descriptor fields used below, in registers
-  const int kx = bd.kind[0], ky = bd.kind[1];
-  const bool ccx = kind_info(kx).cent == CC, ccy = kind_info(ky).cent == CC;
-  const int cnx = bd.cnx, cny = bd.cny, fnx = bd.fnx;
-  const int64_t cplane = (int64_t)cnx * cny, fplane = (int64_t)fnx * bd.fny;
-  const int cnz = (int)(bd.cnp / cplane);
-  const int clo0 = bd.clo[0], clo1 = bd.clo[1], clo2 = bd.clo[2];
-  const int cx0 = clo0 + xt * bd.at[0], cy0 = clo1 + yt * bd.at[1], cz0 = clo2 + zt * bd.at[2];
-  const int txe = min(bd.at[0], clo0 + cnx - cx0), tye = min(bd.at[1], clo1 + cny - cy0);
-  const int cz1 = min(cz0 + bd.at[2] - 1, clo2 + cnz - 1);
-  const int rhx = sep_rhi(kx), dx = rhx - sep_rlo(kx);
-  const int rhy = sep_rhi(ky), dy = rhy - sep_rlo(ky);
-  const int fxo = 2 * (cx0 - rhx), fyo = 2 * (cy0 - rhy);
-  const int fw = 2 * txe + 2 * dx, fh = 2 * tye + 2 * dy;
-  const int fpw = fp_pitch(txe, DM), gpw = g_pitch(tye, DM);
-  const int ax = max(0, bd.rlo[0] - fxo), bx = min(fw - 1, bd.rhi[0] - fxo);
-  const int ay = max(0, bd.rlo[1] - fyo), by = min(fh - 1, bd.rhi[1] - fyo);
-  int fa = max(2 * (cz0 - KZ::RHI), bd.rlo[2]);
-  int fb = min(2 * (cz1 - KZ::RLO) + 1, bd.rhi[2]);
-  if (ax > bx || ay > by) { // no region point in the footprint
-    fa = 1;
-    fb = 0;
-  }
-  const double *fcomp = bd.fine + comp * bd.fnp; // fine_bar component
-  const uint64_t fcomp8 = (uint64_t)(uintptr_t)fcomp >> 3;
-  // element offset of footprint point (0, 0) of fine plane fz in the component
-  const int64_t org = (int64_t)(fyo - bd.flo[1]) * fnx + (fxo - bd.flo[0]) - (int64_t)bd.flo[2] * fplane;
-  const int dpar = (fnx + fpw) & 1; // row r sits at r fpw + ((parity of plane) + r dpar) % 2
-  const bool edge = ax > 0 || bx < fw - 1; // region rows have columns outside the region
-  double *out = bd.cbar + comp * bd.cnp;
-
-  // this thread's columns: y^T source in the x^T result, output offset
-  int ysrc[UPT], cofs[UPT];
-#pragma unroll
-  for (int q = 0; q < UPT; ++q) {
-    const int u = tid + q * NT;
-    const int uj = u / txe, ui = u - uj * txe;
-    ysrc[q] = uj < tye ? ui * gpw + 2 * uj : -1;
-    cofs[q] = (cy0 + uj - clo1) * cnx + (cx0 + ui - clo0);
-  }
-  // this thread's x^T tasks: (segment s, row r), rows fastest
-  int xsrc[XTMAX], xdst[XTMAX], xodd[XTMAX], xn[XTMAX];
-  const int nseg = (txe + XB - 1) / XB;
-#pragma unroll
-  for (int k = 0; k < XTMAX; ++k) {
-    const int t = tid + k * NT;
-    const int s = t / fh, r = t - s * fh;
-    xn[k] = s < nseg ? min(XB, txe - s * XB) : 0;
-    xsrc[k] = r * fpw + 2 * XB * s;
-    xdst[k] = s * XB * gpw + r;
-    xodd[k] = r & dpar;
-  }
-
-  // zero every buffer's footprint once: rows outside the region stay zero;
-  // the columns of region rows outside the region are zeroed with each load
-  for (int k = 0; k < NBUF; ++k)
-    for (int e = tid; e < fh * fpw; e += NT)
-      fbuf[k * FP + e] = 0.0;
-  fence_proxy_async();
-  __syncthreads();
-
-  // issue the copies of fine plane fz into buffer k (the buffer's mbarrier
-  // receives the bulk bytes; thread 0 arrives once every thread has issued)
-  auto load = [&](int fz, int k) {
-    double *S = fbuf + k * FP;
-    const int r = ay + (tid & 31) * (NT / 32) + (tid >> 5); // footprint rows <= NT
-    if (r <= by) {
-      const int64_t rofs = org + (int64_t)fz * fplane + (int64_t)r * fnx; // (r, 0)
-      const int par = (int)((fcomp8 + (uint64_t)rofs) & 1);
-      const int rb = r * fpw + ((par + r * fpw) & 1); // same parity as the row's address
-      const double *rowg = fcomp + rofs;
-      const int c0 = ax + ((par + ax) & 1); // first column with a 16-byte aligned address
-      const int nch = (bx - c0 + 1) >> 1;
-      if (nch > 0) {
-        mbar_expect_tx(mbar + k, 16u * (uint32_t)nch);
-        bulk_g2s(S + rb + c0, rowg + c0, 16u * (uint32_t)nch, mbar + k);
-      }
-      if (c0 > ax)
-        cp_async8(S + rb + ax, rowg + ax);
-      const int cl = c0 + 2 * nch;
-      if (cl <= bx)
-        cp_async8(S + rb + cl, rowg + cl);
-      if (edge) {
-        for (int c = 0; c < ax; ++c)
-          S[rb + c] = 0.0;
-        for (int c = bx + 1; c < fw; ++c)
-          S[rb + c] = 0.0;
-        fence_proxy_async();
-      }
-    }
-  };
-
-  double acc[UPT][L];
-#pragma unroll
-  for (int q = 0; q < UPT; ++q)
-#pragma unroll
-    for (int k = 0; k < L; ++k)
-      acc[q][k] = 0.0;
-  int cc = cz0 - KZ::RHI; // acc[q][k] <-> coarse plane cc + RLO + k
-  auto advance_to = [&](int target) {
-    for (; cc < target; ++cc) {
-      const int cz = cc + KZ::RLO;
-      if (cz >= cz0 && cz <= cz1) {
-        double *o = out + (int64_t)(cz - clo2) * cplane;
-#pragma unroll
-        for (int q = 0; q < UPT; ++q)
-          if (ysrc[q] >= 0)
-            o[cofs[q]] = acc[q][0];
-      }
-#pragma unroll
-      for (int q = 0; q < UPT; ++q) {
-#pragma unroll
-        for (int k = 0; k < L - 1; ++k)
-          acc[q][k] = acc[q][k + 1];
-        acc[q][L - 1] = 0.0;
-      }
-    }
-  };
-
-#pragma unroll
-  for (int d = 0; d < DPF; ++d) {
-    if (fa + d <= fb)
-      load(fa + d, d);
-    cp_async_commit();
-  }
-  __syncthreads();
-  if (tid == 0)
-    for (int d = 0; d < DPF; ++d)
-      if (fa + d <= fb)
-        mbar_arrive(mbar + d);
-  int slot = 0;
-  for (int fz = fa; fz <= fb; ++fz) {
-    int ls = slot + DPF;
-    if (ls >= NBUF)
-      ls -= NBUF;
-    const bool more = fz + DPF <= fb;
-    if (more)
-      load(fz + DPF, ls);
-    cp_async_commit();
-    cp_async_wait_dpf();
-    const uint32_t par = (phase >> slot) & 1u;
-    if (tid == 0 && !mbar_wait_bounded(mbar + slot, par)) {
-      *s_fail = 1;
-      g_adj_timeout = 1;
-    }
-    __syncthreads();
-    if (*s_fail) {
-      // stop: let the copies issued for the next plane land first (bounded)
-      if (tid == 0 && more) {
-        mbar_arrive(mbar + ls);
-        mbar_wait_bounded(mbar + ls, (phase >> ls) & 1u);
-      }
-      cp_async_wait_all();
-      __syncthreads();
-      return false;
-    }
-    if (tid == 0 && more)
-      mbar_arrive(mbar + ls); // every thread issued its copies before the barrier
-    mbar_try(mbar + slot, par); // completed: acquires the bulk data for this thread
-    phase ^= 1u << slot;
-    const double *S = fbuf + slot * FP;
-    const int p0 = (int)((fcomp8 + (uint64_t)(org + (int64_t)fz * fplane)) & 1);
-#pragma unroll
-    for (int k = 0; k < XTMAX; ++k) {
-      if (xn[k] <= 0)
-        continue;
-      const double *src = S + xsrc[k] + ((p0 + xodd[k]) & 1);
-      if (ccx)
-        xt_task<KC>(src, gbuf + xdst[k], gpw, xn[k]);
-      else
-        xt_task<KV>(src, gbuf + xdst[k], gpw, xn[k]);
-    }
-    __syncthreads();
-    advance_to(fz >> 1);
-#pragma unroll
-    for (int q = 0; q < UPT; ++q) {
-      if (ysrc[q] < 0)
-        continue;
-      const double g = ccy ? yt_col<KC>(gbuf + ysrc[q]) : yt_col<KV>(gbuf + ysrc[q]);
-      if (fz & 1)
-        zt_add<KZ, 1, L>(acc[q], g);
-      else
-        zt_add<KZ, 0, L>(acc[q], g);
-    }
-    if (++slot == NBUF)
-      slot = 0;
-  }
-  advance_to(cz1 - KZ::RLO + 1);
-  cp_async_wait_all();
-  __syncthreads(); // the next item reuses the shared buffers
-  return true;
-}
-
-constexpr int BOX_WORDS = (int)(sizeof(BoxDesc) / sizeof(int));
-static_assert(BOX_WORDS <= NT, "one thread per descriptor word");
-
-// Box mode (items == nullptr): the items of box b strided over the grid.
-// Level mode: items of a device work list (sorted by cost, the tiles of a box
-// together) strided over persistent CTAs.
-template <class KV, class KC>
-__global__ void __launch_bounds__(NT, AdjPair<KV, KC>::OCC)
-    adjoint_kernel(const __grid_constant__ BoxDesc b, const BoxDesc *__restrict__ boxes,
-                   const TileRef *__restrict__ items, int nitems) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ BoxDesc box_s;
-  __shared__ uint64_t mbar[NBUF];
-  __shared__ int s_fail;
-  double *fbuf = reinterpret_cast<double *>(smem_raw);
-  double *gbuf = fbuf + NBUF * AdjPair<KV, KC>::FP;
-  if (threadIdx.x == 0) {
-    for (int k = 0; k < NBUF; ++k)
-      mbar_init(mbar + k, 1);
-    mbar_fence_init();
-    s_fail = 0;
-  }
-  __syncthreads();
-  uint32_t phase = 0; // completed-phase parity per buffer
-  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-    const BoxDesc *bp = &b;
-    int xt, yt, zt, comp;
-    if (items) {
-      const TileRef t = items[item];
-      if (threadIdx.x < BOX_WORDS)
-        reinterpret_cast<int *>(&box_s)[threadIdx.x] =
-            reinterpret_cast<const int *>(boxes + t.box)[threadIdx.x];
-      __syncthreads();
-      bp = &box_s;
-      xt = t.tx;
-      yt = t.ty;
-      zt = t.tz;
-      comp = t.comp;
-    } else {
-      int r = item;
-      xt = r % b.ant[0];
-      r /= b.ant[0];
-      yt = r % b.ant[1];
-      r /= b.ant[1];
-      zt = r % b.ant[2];
-      comp = r / b.ant[2];
-    }
-    const bool ok = kind_info(bp->kind[2]).cent == CC
-                        ? adj_item<KV, KC, KC>(fbuf, gbuf, mbar, &s_fail, phase, *bp, xt, yt, zt, comp)
-                        : adj_item<KV, KC, KV>(fbuf, gbuf, mbar, &s_fail, phase, *bp, xt, yt, zt, comp);
-    if (!ok)
-      return;
-    // adj_item ends with a barrier: box_s may be overwritten
-  }
-}
-
-using AdjFn = void (*)(const BoxDesc, const BoxDesc *, const TileRef *, int);
-
-// Kernel and shared-memory size of a pair (nullptr for the nonlinear ones).
-template <class V, class C> AdjFn adj_fn(size_t *smem) {
-  if constexpr (std::is_same_v<C, CcMinmod>) {
+// Kernel and shared-memory size of group 8 pair + centring.
+AdjFn adj_kernel(int group, size_t *smem) {
+  static AdjFn (*const parts[kStreamParts])(int, size_t *) = {
+      adj_kernel_part0, adj_kernel_part1, adj_kernel_part2, adj_kernel_part3,
+      adj_kernel_part4, adj_kernel_part5, adj_kernel_part6, adj_kernel_part7};
+  if (group < 0 || group >= kAdjGroups)
     return nullptr;
-  } else {
-    *smem = AdjPair<V, C>::SMEM;
-    return adjoint_kernel<V, C>;
-  }
-}
-
-AdjFn adj_kernel(int pair, size_t *smem) {
-  switch (pair) {
-#define CXB_ADJ_CASE(I, V, C, KVI, KCI)                                        \
-  case I:                                                                      \
-    return adj_fn<V, C>(smem);
-    CXB_STREAM_PAIRS(CXB_ADJ_CASE)
-#undef CXB_ADJ_CASE
-  default:
-    break;
-  }
-  return nullptr;
+  return parts[group % kStreamParts](group / kStreamParts, smem);
 }
 
 template <class V, class C> int adj_upt_of() {
@@ -522,14 +40,14 @@ int adj_upt(int pair) {
   return 2;
 }
 
-bool g_adj_attr[kStreamPairs] = {};
-int g_adj_grid[kStreamPairs] = {};
+bool g_adj_attr[kAdjGroups] = {};
+int g_adj_grid[kAdjGroups] = {};
 
-// Kernel of a pair, its dynamic shared memory allowed and its persistent
+// Kernel of a group, its dynamic shared memory allowed and its persistent
 // grid (SMs x resident CTAs) recorded on first use.
-AdjFn adj_ready(int pair, size_t *smem) {
-  AdjFn k = pair >= 0 && pair < kStreamPairs ? adj_kernel(pair, smem) : nullptr;
-  if (k && !g_adj_attr[pair]) {
+AdjFn adj_ready(int group, size_t *smem) {
+  AdjFn k = adj_kernel(group, smem);
+  if (k && !g_adj_attr[group]) {
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem) !=
         cudaSuccess)
       return nullptr;
@@ -537,8 +55,8 @@ AdjFn adj_ready(int pair, size_t *smem) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, *smem);
-    g_adj_grid[pair] = sms * (per_sm > 0 ? per_sm : 1);
-    g_adj_attr[pair] = true;
+    g_adj_grid[group] = sms * (per_sm > 0 ? per_sm : 1);
+    g_adj_attr[group] = true;
   }
   return k;
 }
@@ -546,12 +64,18 @@ AdjFn adj_ready(int pair, size_t *smem) {
 } // namespace
 
 int adjoint_take_timeout() {
-  int v = 0, zero = 0;
-  if (cudaMemcpyFromSymbol(&v, g_adj_timeout, sizeof v) != cudaSuccess)
-    return -1;
-  if (v)
-    cudaMemcpyToSymbol(g_adj_timeout, &zero, sizeof zero);
-  return v;
+  static int (*const parts[kStreamParts])() = {adj_timeout_part0, adj_timeout_part1,
+                                               adj_timeout_part2, adj_timeout_part3,
+                                               adj_timeout_part4, adj_timeout_part5,
+                                               adj_timeout_part6, adj_timeout_part7};
+  int any = 0;
+  for (auto f : parts) {
+    const int v = f();
+    if (v < 0)
+      return -1;
+    any |= v;
+  }
+  return any;
 }
 
 int adjoint_pair_of(const BoxDesc &b) {
@@ -559,6 +83,14 @@ int adjoint_pair_of(const BoxDesc &b) {
     if (b.kind[d] == K_CC_MINMOD1 || b.kind[d] == K_CC_ENO2)
       return -1;
   return stream_pair_of(b.kind[0], b.kind[1], b.kind[2]);
+}
+
+int adjoint_group_of(const BoxDesc &b) {
+  const int pair = adjoint_pair_of(b);
+  const int cm = (kind_info(b.kind[0]).cent == CC ? 4 : 0) |
+                 (kind_info(b.kind[1]).cent == CC ? 2 : 0) |
+                 (kind_info(b.kind[2]).cent == CC ? 1 : 0);
+  return pair < 0 ? -1 : kStreamParts * pair + cm;
 }
 
 void adjoint_tiling(BoxDesc &b, int min_items) {
@@ -580,9 +112,9 @@ void adjoint_tiling(BoxDesc &b, int min_items) {
   b.ant[2] = (cnz + b.at[2] - 1) / b.at[2];
 }
 
-int adjoint_level_grid(int pair) {
+int adjoint_level_grid(int group) {
   size_t smem = 0;
-  return adj_ready(pair, &smem) ? g_adj_grid[pair] : 0;
+  return adj_ready(group, &smem) ? g_adj_grid[group] : 0;
 }
 
 cudaError_t launch_prolong_adjoint_box(const BoxDesc &b0, int per_group, double *crse_bar,
@@ -590,28 +122,28 @@ cudaError_t launch_prolong_adjoint_box(const BoxDesc &b0, int per_group, double 
   (void)per_group; // linear operators: per-group and per-variable agree
   if (b0.ncomp <= 0 || b0.cnp <= 0)
     return cudaSuccess;
-  const int pair = adjoint_pair_of(b0);
+  const int group = adjoint_group_of(b0);
   size_t smem = 0;
-  AdjFn k = adj_ready(pair, &smem);
+  AdjFn k = adj_ready(group, &smem);
   if (!k)
     return cudaErrorInvalidValue;
   BoxDesc b = b0;
   b.cbar = crse_bar;
-  adjoint_tiling(b, g_adj_grid[pair]);
+  adjoint_tiling(b, g_adj_grid[group]);
   const int64_t n64 = (int64_t)b.ant[0] * b.ant[1] * b.ant[2] * b.ncomp;
   if (n64 > INT32_MAX)
     return cudaErrorInvalidValue;
   const int n = (int)n64;
-  k<<<n < g_adj_grid[pair] ? n : g_adj_grid[pair], NT, smem, s>>>(b, nullptr, nullptr, n);
+  k<<<n < g_adj_grid[group] ? n : g_adj_grid[group], NT, smem, s>>>(b, nullptr, nullptr, n);
   return cudaGetLastError();
 }
 
-cudaError_t launch_adjoint_level(int pair, const BoxDesc *d_boxes, const TileRef *d_items,
+cudaError_t launch_adjoint_level(int group, const BoxDesc *d_boxes, const TileRef *d_items,
                                  int nitems, int grid, cudaStream_t s) {
   if (nitems <= 0)
     return cudaSuccess;
   size_t smem = 0;
-  AdjFn k = adj_ready(pair, &smem);
+  AdjFn k = adj_ready(group, &smem);
   if (!k)
     return cudaErrorInvalidValue;
   BoxDesc unused{};

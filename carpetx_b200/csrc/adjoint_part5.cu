@@ -1,0 +1,32 @@
+// Adjoint-kernel instantiations of centring 5 ((cx << 2) | (cy << 1) | cz),
+// one per linear stencil pair of stream_pairs.h; split only to compile in
+// parallel.  This file's copy of the timeout flag is read here.
+#include "adjoint_kernel.cuh"
+
+namespace cxb {
+namespace adj {
+
+AdjFn adj_kernel_part5(int pair, size_t *smem) {
+  switch (pair) {
+#define CXB_ADJ_CASE(I, V, C, KVI, KCI)                                        \
+  case I:                                                                      \
+    return adj_fn<V, C, 5>(smem);
+    CXB_STREAM_PAIRS(CXB_ADJ_CASE)
+#undef CXB_ADJ_CASE
+  default:
+    break;
+  }
+  return nullptr;
+}
+
+int adj_timeout_part5() {
+  int v = 0, zero = 0;
+  if (cudaMemcpyFromSymbol(&v, g_adj_timeout, sizeof v) != cudaSuccess)
+    return -1;
+  if (v)
+    cudaMemcpyToSymbol(g_adj_timeout, &zero, sizeof zero);
+  return v;
+}
+
+} // namespace adj
+} // namespace cxb

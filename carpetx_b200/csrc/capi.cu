@@ -468,7 +468,7 @@ int cx_level_plan_create_adjoint(const cx_box_t *boxes, int nboxes, int per_grou
           }
       }
   }
-  auto group_of = [&](const TileRef &t) { return adjoint_pair_of(p->boxes[t.box]); };
+  auto group_of = [&](const TileRef &t) { return adjoint_group_of(p->boxes[t.box]); };
   std::stable_sort(keyed.begin(), keyed.end(),
                    [&](const std::pair<int64_t, TileRef> &a, const std::pair<int64_t, TileRef> &b) {
                      const int ga = group_of(a.second), gb = group_of(b.second);

@@ -104,11 +104,14 @@ void adjoint_tiling(BoxDesc &b, int min_items);
 // Pair index of an operator whose adjoint has a kernel (linear separable),
 // else -1.
 int adjoint_pair_of(const BoxDesc &b);
-int adjoint_level_grid(int pair);
+// Adjoint-kernel instantiation of such an operator: 8 x pair + centring
+// (cx << 2 | cy << 1 | cz); -1 if none.  Below kStrGroups.
+int adjoint_group_of(const BoxDesc &b);
+int adjoint_level_grid(int group);
 // 1 if a bounded wait of the adjoint kernels gave up since the last call
 // (and clears the flag), 0 if not, -1 if the flag could not be read.
 int adjoint_take_timeout();
-cudaError_t launch_adjoint_level(int pair, const BoxDesc *d_boxes,
+cudaError_t launch_adjoint_level(int group, const BoxDesc *d_boxes,
                                  const TileRef *d_items, int nitems, int grid,
                                  cudaStream_t s);
 
