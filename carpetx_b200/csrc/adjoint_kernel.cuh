@@ -284,8 +284,10 @@ __device__ __forceinline__ bool adj_item(double *fbuf, double *gbuf, uint64_t *m
     xodd[k] = r & dpar;
   }
 
-  // zero every buffer's footprint once: rows outside the region stay zero;
-  // the columns of region rows outside the region are zeroed with each load
+  // zero every buffer's footprint once: rows outside the region and the
+  // columns of region rows outside the region stay zero, except the one
+  // column at each end that a copy placed with the other parity wrote (see
+  // load)
   for (int k = 0; k < NBUF; ++k)
     for (int e = tid; e < fh * fpw; e += NT)
       fbuf[k * FP + e] = 0.0;
@@ -314,10 +316,15 @@ __device__ __forceinline__ bool adj_item(double *fbuf, double *gbuf, uint64_t *m
       if (cl <= bx)
         cp_async8(S + rb + cl, rowg + cl);
       if (edge) {
-        for (int c = 0; c < ax; ++c)
-          S[rb + c] = 0.0;
-        for (int c = bx + 1; c < fw; ++c)
-          S[rb + c] = 0.0;
+        // a row sits at r fpw + s + c, s = 0 or 1 by plane; copies write
+        // c in [ax, bx] only, so with s = 1 the column ax - 1 holds what a
+        // plane with s = 0 put at ax, and with s = 0 the column bx + 1 holds
+        // what a plane with s = 1 put at bx; every other column outside the
+        // region keeps the zero of the item's start
+        if (ax > 0)
+          S[rb + ax - 1] = 0.0;
+        if (bx < fw - 1)
+          S[rb + bx + 1] = 0.0;
         fence_proxy_async();
       }
     }
