@@ -22,10 +22,14 @@
 //          The rows are dealt across the warps: a warp's bulk copies are
 //          issued one lane after the other, so spreading them shortens the
 //          issue;
-//   x^T    G(cx, fy) for the tile's coarse x and every footprint row, XB
-//          coarse x per task from a register window of the fine row, into
-//          shared memory (column major: the y taps of a column are adjacent);
-//   y^T    each thread gathers g(cx, cy) of its UPT columns;
+//   y^T    H(fx, cy) for every footprint column and the tile's coarse y,
+//          YB coarse y per task from a register window down the fine column
+//          (consecutive lanes read consecutive fine x of a row), into shared
+//          memory split by the parity of fx; y first, because the tiles are
+//          wider than tall and the first pass pays for the other direction's
+//          halo at fine resolution;
+//   x^T    each thread gathers g(cx, cy) of its UPT columns from H (its taps
+//          are adjacent in the two parity halves);
 //   z^T    each thread accumulates w(off, o) g into the coarse planes
 //          cc + o that fine plane fz = 2 cc + off reaches (a register ring of
 //          L = RHI - RLO + 1 partial sums); when cc moves on, coarse plane
@@ -106,6 +110,14 @@ template <int P> struct Weight<VcCons<P>> {
 template <class K> CXB_HD constexpr double wtap(int m) {
   return Weight<K>::w(m & 1, K::RHI - (m >> 1));
 }
+// partial sum (0 or 1) that tap m joins: the taps of nonzero weight
+// alternate, so two independent FMA chains of equal length
+template <class K> CXB_HD constexpr int wchain(int m) {
+  int n = 0;
+  for (int i = 0; i < m; ++i)
+    n += wtap<K>(i) != 0.0;
+  return n & 1;
+}
 template <class K> constexpr int DK = K::RHI - K::RLO;
 
 // A CTA of NT threads streams a tile of up to NT x UPT coarse columns (at
@@ -119,23 +131,31 @@ constexpr int NT = 256;       // threads per CTA
 constexpr int TMAX = 64;      // tile extent in x or y at most
 constexpr int DPF = 2;        // fine planes prefetched ahead
 constexpr int NBUF = DPF + 1; // shared fine-plane ring
-constexpr int XB = 4;         // coarse x per x^T task
+constexpr int YB = 4;         // coarse y per y^T task
 
 // Footprint of a TX x TY tile for stencil spread D <= DM: rows, row pitch
 // (odd, one more than the widest footprint row: a row is placed at offset 0
-// or 1 to match its global address parity), x^T column pitch (odd).
+// or 1 to match its global address parity).  The y^T result H keeps the
+// even and the odd footprint columns in two halves of TY rows of TX + DM
+// points; the second half starts 8 doubles past a multiple of 16, so the
+// even and odd lanes of a warp's stores fall in different banks.
 CXB_HD constexpr int fp_rows(int ty, int dm) { return 2 * ty + 2 * dm; }
 CXB_HD constexpr int fp_pitch(int tx, int dm) { return 2 * tx + 2 * dm + 1; }
-CXB_HD constexpr int g_pitch(int ty, int dm) { return fp_rows(ty, dm) | 1; }
+CXB_HD constexpr int h_pitch(int tx, int dm) { return tx + dm; }
+CXB_HD constexpr int h_half(int tx, int ty, int dm) {
+  return (ty * h_pitch(tx, dm) + 15) / 16 * 16 + 8;
+}
 CXB_HD constexpr int tile_ty(int tx, int nu) { return nu / tx < TMAX ? nu / tx : TMAX; }
+// what: 0 footprint plane, 1 y^T result, 2 y^T tasks, 3 footprint plane plus
+// the rows the last y^T window of a column may read past it
 CXB_HD constexpr int max_fp(int dm, int nu, int what) {
   int m = 0;
   for (int tx = 1; tx <= TMAX; ++tx) {
     const int ty = tile_ty(tx, nu);
-    const int nseg = (tx + XB - 1) / XB;
     const int v = what == 0   ? fp_rows(ty, dm) * fp_pitch(tx, dm)
-                  : what == 1 ? tx * g_pitch(ty, dm)
-                              : nseg * fp_rows(ty, dm);
+                  : what == 1 ? 2 * h_half(tx, ty, dm)
+                  : what == 2 ? (2 * tx + 2 * dm) * ((ty + YB - 1) / YB)
+                              : (fp_rows(ty, dm) + 2 * YB) * fp_pitch(tx, dm);
     m = v > m ? v : m;
   }
   return m;
@@ -148,13 +168,17 @@ template <class KV, class KC> struct AdjPair {
   static constexpr int UPT = upt_of(DM);
   static constexpr int NU = NT * UPT; // coarse columns per item at most
   static constexpr int FP = (max_fp(DM, NU, 0) + 1) & ~1; // fine footprint plane (even: 16-byte buffers)
-  static constexpr int GP = max_fp(DM, NU, 1);            // x^T result
-  static constexpr int XTMAX = (max_fp(DM, NU, 2) + NT - 1) / NT; // x^T tasks per thread
-  // the last x^T window of a row may run 2 (XB - 1) points past the row
-  static constexpr size_t SMEM = sizeof(double) * (size_t)(NBUF * FP + GP + 2 * XB);
+  static constexpr int GP = max_fp(DM, NU, 1);            // y^T result
+  static constexpr int XTMAX = (max_fp(DM, NU, 2) + NT - 1) / NT; // y^T tasks per thread
+  // the last y^T window of a column may read up to 2 YB - 2 rows past the
+  // footprint (into the next buffer, or into H for the last one; only
+  // results that are not stored use them): the allocation covers them
+  static constexpr int OVER = max_fp(DM, NU, 3) - FP;
+  static constexpr size_t SMEM =
+      sizeof(double) * (size_t)(NBUF * FP + (GP > OVER ? GP : OVER) + 2);
   static_assert(SMEM + 1024 <= 227 * 1024, "shared memory per CTA");
   static constexpr int OCC = SMEM + 2048 <= 113 * 1024 ? 2 : 1; // CTAs per SM
-  static_assert(XTMAX <= 3, "x^T task registers");
+  static_assert(XTMAX <= 3, "y^T task registers");
 };
 
 __device__ __forceinline__ void cp_async8(double *sdst, const double *gsrc) {
@@ -173,19 +197,22 @@ namespace {
 __device__ int g_adj_timeout = 0;
 }
 
-// x^T task: XB coarse x of one footprint row from a register window; only
-// the first n are stored (the window of the last task of a row may run past
-// the row: those points reach only unstored results).
+// y^T task: YB coarse y of one footprint column from a register window
+// down the column; tap i is fine row i of the window, at e + i fpw for even
+// i and o + i fpw for odd i (the two row parities of the footprint).  Only
+// the first n results are stored, hp apart (the window of the last task of
+// a column may run past the footprint: those rows reach only unstored
+// results).
 template <class K>
-__device__ __forceinline__ void xt_task(const double *__restrict__ src, double *__restrict__ dst,
-                                        int gpw, int n) {
-  constexpr int D = DK<K>, WIN = 2 * XB + 2 * D;
+__device__ __forceinline__ void yt_task(const double *__restrict__ e, const double *__restrict__ o,
+                                        int fpw, double *__restrict__ dst, int hp, int n) {
+  constexpr int D = DK<K>, WIN = 2 * YB + 2 * D;
   double v[WIN];
 #pragma unroll
   for (int i = 0; i < WIN; ++i)
-    v[i] = src[i];
+    v[i] = (i & 1 ? o : e)[i * fpw];
 #pragma unroll
-  for (int t = 0; t < XB; ++t) {
+  for (int t = 0; t < YB; ++t) {
     double acc = 0.0;
 #pragma unroll
     for (int m = 0; m <= 2 * D + 1; ++m) {
@@ -194,19 +221,22 @@ __device__ __forceinline__ void xt_task(const double *__restrict__ src, double *
         acc = fma(w, v[2 * t + m], acc);
     }
     if (t < n)
-      dst[t * gpw] = acc;
+      dst[t * hp] = acc;
   }
 }
 
-// y^T of one column: the 2 D + 2 taps are adjacent in the x^T result.
-template <class K> __device__ __forceinline__ double yt_col(const double *__restrict__ src) {
+// x^T of one column from H: tap m is in the half of parity m & 1, m / 2
+// past the column's start.
+template <class K>
+__device__ __forceinline__ double xt_col(const double *__restrict__ h0,
+                                         const double *__restrict__ h1) {
   constexpr int D = DK<K>;
   double acc = 0.0;
 #pragma unroll
   for (int m = 0; m <= 2 * D + 1; ++m) {
     const double w = wtap<K>(m);
     if (w != 0.0)
-      acc = fma(w, src[m], acc);
+      acc = fma(w, (m & 1 ? h1 : h0)[m >> 1], acc);
   }
   return acc;
 }
@@ -245,7 +275,7 @@ __device__ __forceinline__ bool adj_item(double *fbuf, double *gbuf, uint64_t *m
   constexpr int rhy = KY::RHI, dy = DK<KY>;
   const int fxo = 2 * (cx0 - rhx), fyo = 2 * (cy0 - rhy);
   const int fw = 2 * txe + 2 * dx, fh = 2 * tye + 2 * dy;
-  const int fpw = fp_pitch(txe, DM), gpw = g_pitch(tye, DM);
+  const int fpw = fp_pitch(txe, DM), hp = h_pitch(txe, DM), hoff = h_half(txe, tye, DM);
   const int ax = max(0, bd.rlo[0] - fxo), bx = min(fw - 1, bd.rhi[0] - fxo);
   const int ay = max(0, bd.rlo[1] - fyo), by = min(fh - 1, bd.rhi[1] - fyo);
   int fa = max(2 * (cz0 - KZ::RHI), bd.rlo[2]);
@@ -262,26 +292,27 @@ __device__ __forceinline__ bool adj_item(double *fbuf, double *gbuf, uint64_t *m
   const bool edge = ax > 0 || bx < fw - 1; // region rows have columns outside the region
   double *out = bd.cbar + comp * bd.cnp;
 
-  // this thread's columns: y^T source in the x^T result, output offset
-  int ysrc[UPT], cofs[UPT];
+  // this thread's columns: x^T source in H (-1: none), output offset
+  int hsrc[UPT], cofs[UPT];
 #pragma unroll
   for (int q = 0; q < UPT; ++q) {
     const int u = tid + q * NT;
     const int uj = u / txe, ui = u - uj * txe;
-    ysrc[q] = uj < tye ? ui * gpw + 2 * uj : -1;
+    hsrc[q] = uj < tye ? uj * hp + ui : -1;
     cofs[q] = (cy0 + uj - clo1) * cnx + (cx0 + ui - clo0);
   }
-  // this thread's x^T tasks: (segment s, row r), rows fastest
-  int xsrc[XTMAX], xdst[XTMAX], xodd[XTMAX], xn[XTMAX];
-  const int nseg = (txe + XB - 1) / XB;
+  // this thread's y^T tasks: (footprint column c, group g of YB coarse y),
+  // columns fastest; source offset of the window's first row (before the
+  // plane's row shift), destination in H, results to store (0: none)
+  int ysrc[XTMAX], ydst[XTMAX], yn[XTMAX];
+  const int ngrp = (tye + YB - 1) / YB;
 #pragma unroll
   for (int k = 0; k < XTMAX; ++k) {
     const int t = tid + k * NT;
-    const int s = t / fh, r = t - s * fh;
-    xn[k] = s < nseg ? min(XB, txe - s * XB) : 0;
-    xsrc[k] = r * fpw + 2 * XB * s;
-    xdst[k] = s * XB * gpw + r;
-    xodd[k] = r & dpar;
+    const int g = t / fw, c = t - g * fw;
+    yn[k] = g < ngrp ? min(YB, tye - g * YB) : 0;
+    ysrc[k] = 2 * YB * g * fpw + c;
+    ydst[k] = (c & 1) * hoff + g * YB * hp + (c >> 1);
   }
 
   // zero every buffer's footprint once: rows outside the region and the
@@ -294,16 +325,24 @@ __device__ __forceinline__ bool adj_item(double *fbuf, double *gbuf, uint64_t *m
   fence_proxy_async();
   __syncthreads();
 
+  // this thread's footprint row (rows are dealt across the warps: a warp's
+  // bulk copies are issued one lane after the other) and its element offset
+  // and address parity at fine plane 0
+  const int lr = ay + (tid & 31) * (NT / 32) + (tid >> 5); // footprint rows <= NT
+  const bool has_row = lr <= by;
+  const int64_t rofs0 = org + (int64_t)lr * fnx;
+  const int rpar0 = (int)((fcomp8 + (uint64_t)rofs0) & 1);
+  const int fpl_odd = (int)(fplane & 1);
+  const int rbase = lr * fpw;
+
   // issue the copies of fine plane fz into buffer k (the buffer's mbarrier
   // receives the bulk bytes; thread 0 arrives once every thread has issued)
   auto load = [&](int fz, int k) {
     double *S = fbuf + k * FP;
-    const int r = ay + (tid & 31) * (NT / 32) + (tid >> 5); // footprint rows <= NT
-    if (r <= by) {
-      const int64_t rofs = org + (int64_t)fz * fplane + (int64_t)r * fnx; // (r, 0)
-      const int par = (int)((fcomp8 + (uint64_t)rofs) & 1);
-      const int rb = r * fpw + ((par + r * fpw) & 1); // same parity as the row's address
-      const double *rowg = fcomp + rofs;
+    if (has_row) {
+      const int par = rpar0 ^ (fz & fpl_odd);
+      const int rb = rbase + ((par + rbase) & 1); // same parity as the row's address
+      const double *rowg = fcomp + rofs0 + (int64_t)fz * fplane;
       const int c0 = ax + ((par + ax) & 1); // first column with a 16-byte aligned address
       const int nch = (bx - c0 + 1) >> 1;
       if (nch > 0) {
@@ -344,7 +383,7 @@ __device__ __forceinline__ bool adj_item(double *fbuf, double *gbuf, uint64_t *m
         double *o = out + (int64_t)(cz - clo2) * cplane;
 #pragma unroll
         for (int q = 0; q < UPT; ++q)
-          if (ysrc[q] >= 0)
+          if (hsrc[q] >= 0)
             o[cofs[q]] = acc[q][0];
       }
 #pragma unroll
@@ -399,21 +438,23 @@ __device__ __forceinline__ bool adj_item(double *fbuf, double *gbuf, uint64_t *m
     mbar_try(mbar + slot, par); // completed: acquires the bulk data for this thread
     phase ^= 1u << slot;
     const double *S = fbuf + slot * FP;
+    // row shifts of the plane: row r sits at r fpw + (p0 + r dpar) % 2
     const int p0 = (int)((fcomp8 + (uint64_t)(org + (int64_t)fz * fplane)) & 1);
+    const int se = p0, so = (p0 + dpar) & 1;
 #pragma unroll
     for (int k = 0; k < XTMAX; ++k) {
-      if (xn[k] <= 0)
+      if (yn[k] <= 0)
         continue;
-      const double *src = S + xsrc[k] + ((p0 + xodd[k]) & 1);
-      xt_task<KX>(src, gbuf + xdst[k], gpw, xn[k]);
+      const double *src = S + ysrc[k];
+      yt_task<KY>(src + se, src + so, fpw, gbuf + ydst[k], hp, yn[k]);
     }
     __syncthreads();
     advance_to(fz >> 1);
 #pragma unroll
     for (int q = 0; q < UPT; ++q) {
-      if (ysrc[q] < 0)
+      if (hsrc[q] < 0)
         continue;
-      const double g = yt_col<KY>(gbuf + ysrc[q]);
+      const double g = xt_col<KX>(gbuf + hsrc[q], gbuf + hoff + hsrc[q]);
       if (fz & 1)
         zt_add<KZ, 1, L>(acc[q], g);
       else
