@@ -131,7 +131,7 @@ constexpr int NT = 256;       // threads per CTA
 constexpr int TMAX = 64;      // tile extent in x or y at most
 constexpr int DPF = 2;        // fine planes prefetched ahead
 constexpr int NBUF = DPF + 1; // shared fine-plane ring
-constexpr int YB = 4;         // coarse y per y^T task
+constexpr int YB = 6;         // coarse y per y^T task
 
 // Footprint of a TX x TY tile for stencil spread D <= DM: rows, row pitch
 // (odd, one more than the widest footprint row: a row is placed at offset 0
