@@ -138,8 +138,9 @@ typedef struct cx_level_plan *cx_level_plan_t;
 int cx_level_plan_create(const cx_box_t *boxes, int nboxes, int per_group,
                          cx_level_plan_t *out);
 /* Enqueues the whole level transfer on stream: one persistent launch per
- * kernel family present (separable / limited).  Allocates nothing and does
- * not synchronise, so it can be captured into a CUDA graph. */
+ * separable kernel instantiation present (stencil pair and centring), then
+ * the limited operators' launches.  Allocates nothing and does not
+ * synchronise, so it can be captured into a CUDA graph. */
 int cx_level_plan_execute(cx_level_plan_t plan, cx_stream_t stream);
 /* Number of tiles and fine points (summed over components) in the plan. */
 int cx_level_plan_stats(cx_level_plan_t plan, int64_t *ntiles,
@@ -149,10 +150,10 @@ int cx_level_plan_destroy(cx_level_plan_t plan);
 /* A level plan for the adjoint: executing it overwrites every box's crse
  * array (whole coarse box, every component) with P^T of its fine array,
  * reading the fine array only inside the region, as cx_prolong_adjoint_box
- * does box by box; one persistent launch per stencil pair.  Validation is
- * cx_prolong_box's; operators without a linear separable form (ENO, minmod,
- * active linear fallback) give CX_EUNSUPPORTED.  Executed, destroyed and
- * queried like any level plan. */
+ * does box by box; one persistent launch per stencil pair and centring
+ * present.  Validation is cx_prolong_box's; operators without a linear
+ * separable form (ENO, minmod, active linear fallback) give
+ * CX_EUNSUPPORTED.  Executed, destroyed and queried like any level plan. */
 int cx_level_plan_create_adjoint(const cx_box_t *boxes, int nboxes,
                                  int per_group, cx_level_plan_t *out);
 
