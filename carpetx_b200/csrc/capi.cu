@@ -527,13 +527,16 @@ int cx_level_plan_execute(cx_level_plan_t p, cx_stream_t stream) {
     }
     return CX_OK;
   }
+  bool after_level = false;
   for (int g = 0; g < kStrGroups; ++g) {
     const int n = p->group_off[g + 1] - p->group_off[g];
-    if (n > 0)
+    if (n > 0) {
       if (int e = cuda_status(launch_stream_level(g, p->d_boxes, p->d_tiles + p->group_off[g], n,
-                                                  p->group_grid[g], s),
+                                                  p->group_grid[g], s, after_level),
                               "level launch"))
         return e;
+      after_level = true;
+    }
   }
   for (int id : p->point_boxes)
     if (int e = cuda_status(launch_point_box(p->boxes[id], p->per_group, nullptr, nullptr, s),

@@ -59,10 +59,12 @@ int stream_pair_of(int kx, int ky, int kz);
 int stream_group_of(int kx, int ky, int kz);
 constexpr int kStrGroups = 136; // number of instantiations (8 x kStreamPairs)
 // Level launch of the items of one instantiation; d_items holds only items
-// of boxes served by that group.
+// of boxes served by that group.  after_level: the launch directly follows
+// another level launch of the same transfer on s (boxes disjoint), and may
+// start while that one finishes (programmatic dependent launch).
 cudaError_t launch_stream_level(int group, const BoxDesc *d_boxes,
                                 const TileRef *d_items, int nitems, int grid,
-                                cudaStream_t s);
+                                cudaStream_t s, bool after_level);
 int stream_level_grid(int group);
 // Fills the streaming-kernel tiling of a box (tbase, ntile, zchunk, xcw,
 // npr, upi); min_items > 0 shortens the z chunks of a box launched alone so

@@ -170,7 +170,8 @@ extern "C" int cx_level_execute_noalloc(const cx_box_t *boxes, int nboxes, int p
   for (int g = 0; e == cudaSuccess && g < kStrGroups; ++g) {
     const int n = off[g + 1] - off[g];
     if (n > 0)
-      e = launch_stream_level(g, dev->boxes, dev->items + off[g], n, stream_level_grid(g), s);
+      e = launch_stream_level(g, dev->boxes, dev->items + off[g], n, stream_level_grid(g), s,
+                              false);
   }
   for (int id = 0; e == cudaSuccess && id < nb; ++id)
     if (point[id])

@@ -383,9 +383,18 @@ __global__ void __launch_bounds__(NTS, Kinds<KV, KC, CM>::ZHI - Kinds<KV, KC, CM
     }
     return;
   }
+  // Level launches after the first of a plan are programmatic dependents of
+  // the previous one (they write other boxes): let the next launch start as
+  // soon as every CTA of this one is running, so it fills this launch's
+  // tail, and end with the wait on the previous launch, so that this
+  // launch completes only after it.  Without the launch attribute both
+  // instructions are no-ops.
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   int cur = blockIdx.x;
-  if (cur >= nitems)
+  if (cur >= nitems) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     return;
+  }
   TileRef t_cur = items[cur];
   int w_cur =
       threadIdx.x < BOX_WORDS ? reinterpret_cast<const int *>(boxes + t_cur.box)[threadIdx.x] : 0;
@@ -407,8 +416,10 @@ __global__ void __launch_bounds__(NTS, Kinds<KV, KC, CM>::ZHI - Kinds<KV, KC, CM
         t_next2 = items[nxt + gridDim.x];
     }
     run_item<KV, KC, CM>(sh, box_s, t_cur.tx, t_cur.ty, t_cur.tz, t_cur.comp);
-    if (nxt >= nitems)
+    if (nxt >= nitems) {
+      asm volatile("griddepcontrol.wait;" ::: "memory");
       break;
+    }
     cur = nxt;
     t_cur = t_next;
     t_next = t_next2;

@@ -144,7 +144,7 @@ cudaError_t launch_stream_box(const BoxDesc &b, cudaStream_t s) {
 }
 
 cudaError_t launch_stream_level(int group, const BoxDesc *d_boxes, const TileRef *d_items,
-                                int nitems, int grid, cudaStream_t s) {
+                                int nitems, int grid, cudaStream_t s, bool after_level) {
   using namespace stream;
   if (nitems <= 0)
     return cudaSuccess;
@@ -152,8 +152,17 @@ cudaError_t launch_stream_level(int group, const BoxDesc *d_boxes, const TileRef
   if (!k)
     return cudaErrorInvalidValue;
   BoxDesc unused{};
-  k<<<grid < nitems ? grid : nitems, NTS, sizeof(Shared), s>>>(unused, d_boxes, d_items, nitems);
-  return cudaGetLastError();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid < nitems ? grid : nitems);
+  cfg.blockDim = dim3(NTS);
+  cfg.dynamicSmemBytes = sizeof(Shared);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = after_level ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k, unused, d_boxes, d_items, nitems);
 }
 
 } // namespace cxb
