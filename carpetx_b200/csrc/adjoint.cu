@@ -139,7 +139,7 @@ cudaError_t launch_prolong_adjoint_box(const BoxDesc &b0, int per_group, double 
 }
 
 cudaError_t launch_adjoint_level(int group, const BoxDesc *d_boxes, const TileRef *d_items,
-                                 int nitems, int grid, cudaStream_t s) {
+                                 int nitems, int grid, cudaStream_t s, bool after_level) {
   if (nitems <= 0)
     return cudaSuccess;
   size_t smem = 0;
@@ -147,8 +147,17 @@ cudaError_t launch_adjoint_level(int group, const BoxDesc *d_boxes, const TileRe
   if (!k)
     return cudaErrorInvalidValue;
   BoxDesc unused{};
-  k<<<grid < nitems ? grid : nitems, NT, smem, s>>>(unused, d_boxes, d_items, nitems);
-  return cudaGetLastError();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid < nitems ? grid : nitems);
+  cfg.blockDim = dim3(NT);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = after_level ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k, unused, d_boxes, d_items, nitems);
 }
 
 } // namespace cxb

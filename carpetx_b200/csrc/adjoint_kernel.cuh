@@ -486,6 +486,10 @@ __global__ void __launch_bounds__(NT, AdjPair<KV, KC>::OCC)
   __shared__ int s_fail;
   double *fbuf = reinterpret_cast<double *>(smem_raw);
   double *gbuf = fbuf + NBUF * AdjPair<KV, KC>::FP;
+  // level launches after the first of a plan start in the previous one's
+  // tail and wait for it at their end (programmatic dependent launch; no-ops
+  // without the launch attribute)
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   if (threadIdx.x == 0) {
     for (int k = 0; k < NBUF; ++k)
       mbar_init(mbar + k, 1);
@@ -523,9 +527,10 @@ __global__ void __launch_bounds__(NT, AdjPair<KV, KC>::OCC)
     const bool ok =
         adj_item<KV, KC, KX, KY, KZ>(fbuf, gbuf, mbar, &s_fail, phase, *bp, xt, yt, zt, comp);
     if (!ok)
-      return;
+      break;
     // adj_item ends with a barrier: box_s may be overwritten
   }
+  asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 using AdjFn = void (*)(const BoxDesc, const BoxDesc *, const TileRef *, int);

@@ -517,13 +517,16 @@ int cx_level_plan_execute(cx_level_plan_t p, cx_stream_t stream) {
     for (auto &z : p->zero_boxes)
       if (int e = cuda_status(cudaMemsetAsync(z.first, 0, z.second, s), "memset"))
         return e;
+    bool after_level = false;
     for (int g = 0; g < kStrGroups; ++g) {
       const int n = p->group_off[g + 1] - p->group_off[g];
-      if (n > 0)
+      if (n > 0) {
         if (int e = cuda_status(launch_adjoint_level(g, p->d_boxes, p->d_tiles + p->group_off[g],
-                                                     n, p->group_grid[g], s),
+                                                     n, p->group_grid[g], s, after_level),
                                 "adjoint level launch"))
           return e;
+        after_level = true;
+      }
     }
     return CX_OK;
   }
