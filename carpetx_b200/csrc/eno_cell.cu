@@ -30,6 +30,7 @@ constexpr int EW = ET + 4;      // window edge: tile plus 2 cells each side
 constexpr int EW3 = EW * EW * EW;
 constexpr int ENT = 256;        // threads per CTA
 constexpr int ECPT = ET * ET * ET / ENT; // cells per thread
+constexpr int NWIN = (EW3 + ENT - 1) / ENT; // window points per thread
 
 struct EnoShared {
   double c[EW3];    // coarse window of one component
@@ -76,6 +77,14 @@ __global__ void __launch_bounds__(ENT, 2)
   const int64_t rnp = (int64_t)rnx * rny * (b.rhi[2] - b.rlo[2] + 1);
   const int64_t cplane = (int64_t)b.cnx * b.cny, fplane = (int64_t)b.fnx * b.fny;
   const int ntiles = t.nt[0] * t.nt[1] * t.nt[2];
+  // this thread's window points e = tid + n ENT: (i, j, k) packed 8 bits
+  // each (-1: none), decoded once
+  int wpt[NWIN];
+#pragma unroll
+  for (int n = 0; n < NWIN; ++n) {
+    const int e = tid + n * ENT;
+    wpt[n] = e < EW3 ? (e % EW) | ((e / EW) % EW) << 8 | (e / (EW * EW)) << 16 : -1;
+  }
   for (int item = blockIdx.x; item < ntiles * t.nblk; item += gridDim.x) {
     const int tile = item % ntiles, blk = item / ntiles;
     const int tx = tile % t.nt[0], ty = (tile / t.nt[0]) % t.nt[1], tz = tile / (t.nt[0] * t.nt[1]);
@@ -87,8 +96,12 @@ __global__ void __launch_bounds__(ENT, 2)
     // reads (the rest of the window reaches only cells outside the region)
     auto load = [&](int comp) {
       const double *cb = b.crse + comp * b.cnp;
-      for (int e = tid; e < EW3; e += ENT) {
-        const int i = e % EW, j = (e / EW) % EW, k = e / (EW * EW);
+#pragma unroll
+      for (int n = 0; n < NWIN; ++n) {
+        if (wpt[n] < 0)
+          continue;
+        const int e = tid + n * ENT;
+        const int i = wpt[n] & 255, j = (wpt[n] >> 8) & 255, k = wpt[n] >> 16;
         const int gi = o0 + i, gj = o1 + j, gk = o2 + k;
         if (gi >= b.nlo[0] && gi <= b.nhi[0] && gj >= b.nlo[1] && gj <= b.nhi[1] &&
             gk >= b.nlo[2] && gk <= b.nhi[2])
@@ -104,8 +117,12 @@ __global__ void __launch_bounds__(ENT, 2)
       __syncthreads();
       load(comp);
       __syncthreads();
-      for (int e = tid; e < EW3; e += ENT) {
-        const int i = e % EW, j = (e / EW) % EW, k = e / (EW * EW);
+#pragma unroll
+      for (int n = 0; n < NWIN; ++n) {
+        if (wpt[n] < 0)
+          continue;
+        const int e = tid + n * ENT;
+        const int i = wpt[n] & 255, j = (wpt[n] >> 8) & 255, k = wpt[n] >> 16;
         if (i >= 1 && i <= EW - 2)
           sh.d[0][e] = fmax(sh.d[0][e], fabs(undiv2(sh.c[e - 1], sh.c[e], sh.c[e + 1])));
         if (j >= 1 && j <= EW - 2)
@@ -122,15 +139,23 @@ __global__ void __launch_bounds__(ENT, 2)
       // window axes of direction d: (y, z) for x, (x, z) for y, (x, y) for z
       const int SA_d = d == 0 ? EW : 1;
       const int SB_d = d == 2 ? EW : EW * EW;
-      for (int e = tid; e < EW3; e += ENT) {
-        const int i = e % EW, j = (e / EW) % EW, k = e / (EW * EW);
+#pragma unroll
+      for (int n = 0; n < NWIN; ++n) {
+        if (wpt[n] < 0)
+          continue;
+        const int e = tid + n * ENT;
+        const int i = wpt[n] & 255, j = (wpt[n] >> 8) & 255;
         const int a = d == 0 ? j : i;
         if (a >= 1 && a <= EW - 2)
           sh.t[e] = fmax(fmax(sh.d[d][e - SA_d], sh.d[d][e]), sh.d[d][e + SA_d]);
       }
       __syncthreads();
-      for (int e = tid; e < EW3; e += ENT) {
-        const int i = e % EW, j = (e / EW) % EW, k = e / (EW * EW);
+#pragma unroll
+      for (int n = 0; n < NWIN; ++n) {
+        if (wpt[n] < 0)
+          continue;
+        const int e = tid + n * ENT;
+        const int i = wpt[n] & 255, j = (wpt[n] >> 8) & 255, k = wpt[n] >> 16;
         if (i >= 1 && i <= EW - 2 && j >= 1 && j <= EW - 2 && k >= 1 && k <= EW - 2) {
           const double w = fmax(fmax(sh.t[e - SB_d], sh.t[e]), sh.t[e + SB_d]);
           sh.m[e] = d == 0 ? w : fmax(sh.m[e], w);
@@ -148,12 +173,16 @@ __global__ void __launch_bounds__(ENT, 2)
       cell[q] = widx(ci + 2, cj + 2, ck + 2);
       double min_dd = __longlong_as_double(0x7ff0000000000000LL); // +inf
       int bx = 0, by = 0, bz = 0;
+#pragma unroll
       for (int sk = -1; sk <= 1; ++sk)
+#pragma unroll
         for (int sj = -1; sj <= 1; ++sj)
 #pragma unroll
           for (int si = -1; si <= 1; ++si) {
-            // 1 + sqrt(DBL_EPSILON) * |s|_1, sqrt(2^-52) = 2^-26 exactly
-            const double pen = fadd(1.0, fmul(0x1p-26, (double)(abs(si) + abs(sj) + abs(sk))));
+            // 1 + sqrt(DBL_EPSILON) * |s|_1 with sqrt(2^-52) = 2^-26: exact
+            // for |s|_1 <= 3, a constant per candidate
+            const int n1 = (si != 0) + (sj != 0) + (sk != 0);
+            const double pen = 1.0 + 0x1p-26 * n1;
             const double dd = fmul(pen, sh.m[cell[q] + si + EW * sj + EW * EW * sk]);
             if (dd < min_dd) {
               min_dd = dd;
