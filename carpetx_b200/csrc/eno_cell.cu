@@ -32,11 +32,21 @@ constexpr int ENT = 256;        // threads per CTA
 constexpr int ECPT = ET * ET * ET / ENT; // cells per thread
 constexpr int NWIN = (EW3 + ENT - 1) / ENT; // window points per thread
 
+// Guard points before the first and after the last window array: the
+// passes below evaluate every window point with neighbours up to EW^2 away,
+// without bounds tests; the values at the window's faces that read across
+// an array end are garbage, and they reach no M(p) with p in [1, EW - 2]^3
+// (the only points the search reads).
+constexpr int EPAD = EW * EW + EW + 1;
+
 struct EnoShared {
+  double pad0[EPAD];
   double c[EW3];    // coarse window of one component
   double d[3][EW3]; // |undivided differences| per direction (max over the block's components)
-  double t[EW3];    // window maximum along the first axis
+  double a[EW3];    // A: max over z of D_x
+  double b[EW3];    // B: max(max over z of D_y, max over y of D_z)
   double m[EW3];    // M(p)
+  double pad1[EPAD];
 };
 
 __device__ __forceinline__ int widx(int i, int j, int k) { return (k * EW + j) * EW + i; }
@@ -72,6 +82,12 @@ __global__ void __launch_bounds__(ENT, 2)
                     signed char *shifts, unsigned char *fallback) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   EnoShared &sh = *reinterpret_cast<EnoShared *>(smem_raw);
+  // the window arrays as one run of doubles, guards included, for the
+  // neighbour reads across array ends
+  double *const wbuf = reinterpret_cast<double *>(smem_raw);
+  double *const C = wbuf + EPAD;
+  double *const D0 = C + EW3, *const D1 = D0 + EW3, *const D2 = D1 + EW3;
+  double *const A = D2 + EW3, *const B = A + EW3, *const Mw = B + EW3;
   const int tid = threadIdx.x;
   const int rnx = b.rhi[0] - b.rlo[0] + 1, rny = b.rhi[1] - b.rlo[1] + 1;
   const int64_t rnp = (int64_t)rnx * rny * (b.rhi[2] - b.rlo[2] + 1);
@@ -111,58 +127,55 @@ __global__ void __launch_bounds__(ENT, 2)
     };
 
     // D_d = max over the block's components of |undivided difference in d|
-    for (int e = tid; e < 3 * EW3; e += ENT)
-      (&sh.d[0][0])[e] = 0.0;
+    // (valid where the difference's three points are in the window)
     for (int comp = c0; comp < c1; ++comp) {
       __syncthreads();
       load(comp);
       __syncthreads();
 #pragma unroll
       for (int n = 0; n < NWIN; ++n) {
-        if (wpt[n] < 0)
-          continue;
         const int e = tid + n * ENT;
-        const int i = wpt[n] & 255, j = (wpt[n] >> 8) & 255, k = wpt[n] >> 16;
-        if (i >= 1 && i <= EW - 2)
-          sh.d[0][e] = fmax(sh.d[0][e], fabs(undiv2(sh.c[e - 1], sh.c[e], sh.c[e + 1])));
-        if (j >= 1 && j <= EW - 2)
-          sh.d[1][e] = fmax(sh.d[1][e], fabs(undiv2(sh.c[e - EW], sh.c[e], sh.c[e + EW])));
-        if (k >= 1 && k <= EW - 2)
-          sh.d[2][e] = fmax(sh.d[2][e], fabs(undiv2(sh.c[e - EW * EW], sh.c[e], sh.c[e + EW * EW])));
+        if (e >= EW3)
+          break;
+        const double cx = fabs(undiv2(C[e - 1], C[e], C[e + 1]));
+        const double cy = fabs(undiv2(C[e - EW], C[e], C[e + EW]));
+        const double cz = fabs(undiv2(C[e - EW * EW], C[e], C[e + EW * EW]));
+        if (comp == c0) {
+          D0[e] = cx;
+          D1[e] = cy;
+          D2[e] = cz;
+        } else {
+          D0[e] = fmax(D0[e], cx);
+          D1[e] = fmax(D1[e], cy);
+          D2[e] = fmax(D2[e], cz);
+        }
       }
     }
     __syncthreads();
-    // M(p) = max over d of the 3 x 3 window maximum of D_d across d, for
-    // p in [1, EW - 2]^3 (the shifted cells the search visits)
+    // M(p) = max over d of the 3 x 3 window maximum of D_d across d
+    //      = max(W_y(A), W_x(B)),  A = W_z(D_x),  B = max(W_z(D_y), W_y(D_z)),
+    // with W_a the maximum over a -1, 0, +1 along axis a (fmax is exact, so
+    // the regrouping gives the same value); valid for p in [1, EW - 2]^3
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      // window axes of direction d: (y, z) for x, (x, z) for y, (x, y) for z
-      const int SA_d = d == 0 ? EW : 1;
-      const int SB_d = d == 2 ? EW : EW * EW;
-#pragma unroll
-      for (int n = 0; n < NWIN; ++n) {
-        if (wpt[n] < 0)
-          continue;
-        const int e = tid + n * ENT;
-        const int i = wpt[n] & 255, j = (wpt[n] >> 8) & 255;
-        const int a = d == 0 ? j : i;
-        if (a >= 1 && a <= EW - 2)
-          sh.t[e] = fmax(fmax(sh.d[d][e - SA_d], sh.d[d][e]), sh.d[d][e + SA_d]);
-      }
-      __syncthreads();
-#pragma unroll
-      for (int n = 0; n < NWIN; ++n) {
-        if (wpt[n] < 0)
-          continue;
-        const int e = tid + n * ENT;
-        const int i = wpt[n] & 255, j = (wpt[n] >> 8) & 255, k = wpt[n] >> 16;
-        if (i >= 1 && i <= EW - 2 && j >= 1 && j <= EW - 2 && k >= 1 && k <= EW - 2) {
-          const double w = fmax(fmax(sh.t[e - SB_d], sh.t[e]), sh.t[e + SB_d]);
-          sh.m[e] = d == 0 ? w : fmax(sh.m[e], w);
-        }
-      }
-      __syncthreads();
+    for (int n = 0; n < NWIN; ++n) {
+      const int e = tid + n * ENT;
+      if (e >= EW3)
+        break;
+      constexpr int Z = EW * EW;
+      A[e] = fmax(fmax(D0[e - Z], D0[e]), D0[e + Z]);
+      B[e] = fmax(fmax(fmax(D1[e - Z], D1[e]), D1[e + Z]),
+                  fmax(fmax(D2[e - EW], D2[e]), D2[e + EW]));
     }
+    __syncthreads();
+#pragma unroll
+    for (int n = 0; n < NWIN; ++n) {
+      const int e = tid + n * ENT;
+      if (e >= EW3)
+        break;
+      Mw[e] = fmax(fmax(fmax(A[e - EW], A[e]), A[e + EW]),
+                   fmax(fmax(B[e - 1], B[e]), B[e + 1]));
+    }
+    __syncthreads();
 
     // shift search per cell: first minimum in the reference's order
     int cell[ECPT], shx[ECPT], shy[ECPT], shz[ECPT];
