@@ -46,6 +46,7 @@ struct EnoShared {
   double a[EW3];    // A: max over z of D_x
   double b[EW3];    // B: max(max over z of D_y, max over y of D_z)
   double m[EW3];    // M(p)
+  double p[EW3];    // the other coarse window buffer (the next item's, prefetched)
   double pad1[EPAD];
 };
 
@@ -88,6 +89,10 @@ __global__ void __launch_bounds__(ENT, 2)
   double *const C = wbuf + EPAD;
   double *const D0 = C + EW3, *const D1 = D0 + EW3, *const D2 = D1 + EW3;
   double *const A = D2 + EW3, *const B = A + EW3, *const Mw = B + EW3;
+  // the coarse window alternates between c and p: while an item evaluates
+  // its children, the first window of the next item is copied into the other
+  // buffer with cp.async
+  double *Cc = C, *Cn = Mw + EW3;
   const int tid = threadIdx.x;
   const int rnx = b.rhi[0] - b.rlo[0] + 1, rny = b.rhi[1] - b.rlo[1] + 1;
   const int64_t rnp = (int64_t)rnx * rny * (b.rhi[2] - b.rlo[2] + 1);
@@ -101,45 +106,71 @@ __global__ void __launch_bounds__(ENT, 2)
     const int e = tid + n * ENT;
     wpt[n] = e < EW3 ? (e % EW) | ((e / EW) % EW) << 8 | (e / (EW * EW)) << 16 : -1;
   }
-  for (int item = blockIdx.x; item < ntiles * t.nblk; item += gridDim.x) {
-    const int tile = item % ntiles, blk = item / ntiles;
+  const int nitems = ntiles * t.nblk;
+  // window origin (coarse index of local 0) and first component of an item
+  auto origin = [&](int item, int &o0, int &o1, int &o2, int &blk) {
+    const int tile = item % ntiles;
+    blk = item / ntiles;
     const int tx = tile % t.nt[0], ty = (tile / t.nt[0]) % t.nt[1], tz = tile / (t.nt[0] * t.nt[1]);
-    // window origin (coarse index of local 0) and the block's components
-    const int o0 = t.clo[0] + tx * ET - 2, o1 = t.clo[1] + ty * ET - 2, o2 = t.clo[2] + tz * ET - 2;
-    const int c0 = per_group ? 0 : blk, c1 = per_group ? b.ncomp : blk + 1;
-
-    // load the window of component comp: the coarse points the operator
-    // reads (the rest of the window reaches only cells outside the region)
-    auto load = [&](int comp) {
-      const double *cb = b.crse + comp * b.cnp;
+    o0 = t.clo[0] + tx * ET - 2;
+    o1 = t.clo[1] + ty * ET - 2;
+    o2 = t.clo[2] + tz * ET - 2;
+  };
+  // copy the window at origin (o0, o1, o2) of component comp into W: the
+  // coarse points the operator reads (the rest of the window reaches only
+  // cells outside the region); asynchronous (cp.async) or plain loads
+  auto load = [&](double *W, int o0, int o1, int o2, int comp, bool async) {
+    const double *cb = b.crse + comp * b.cnp;
 #pragma unroll
-      for (int n = 0; n < NWIN; ++n) {
-        if (wpt[n] < 0)
-          continue;
-        const int e = tid + n * ENT;
-        const int i = wpt[n] & 255, j = (wpt[n] >> 8) & 255, k = wpt[n] >> 16;
-        const int gi = o0 + i, gj = o1 + j, gk = o2 + k;
-        if (gi >= b.nlo[0] && gi <= b.nhi[0] && gj >= b.nlo[1] && gj <= b.nhi[1] &&
-            gk >= b.nlo[2] && gk <= b.nhi[2])
-          sh.c[e] = __ldg(cb + (gi - b.clo[0]) + (int64_t)b.cnx * (gj - b.clo[1]) +
-                          cplane * (gk - b.clo[2]));
+    for (int n = 0; n < NWIN; ++n) {
+      if (wpt[n] < 0)
+        continue;
+      const int e = tid + n * ENT;
+      const int i = wpt[n] & 255, j = (wpt[n] >> 8) & 255, k = wpt[n] >> 16;
+      const int gi = o0 + i, gj = o1 + j, gk = o2 + k;
+      if (gi >= b.nlo[0] && gi <= b.nhi[0] && gj >= b.nlo[1] && gj <= b.nhi[1] &&
+          gk >= b.nlo[2] && gk <= b.nhi[2]) {
+        const double *src =
+            cb + (gi - b.clo[0]) + (int64_t)b.cnx * (gj - b.clo[1]) + cplane * (gk - b.clo[2]);
+        if (async)
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(
+                           (unsigned)__cvta_generic_to_shared(W + e)),
+                       "l"(src)
+                       : "memory");
+        else
+          W[e] = __ldg(src);
       }
-    };
+    }
+  };
+  if (blockIdx.x < nitems) {
+    int o0, o1, o2, blk;
+    origin(blockIdx.x, o0, o1, o2, blk);
+    load(Cc, o0, o1, o2, per_group ? 0 : blk, true);
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+    int o0, o1, o2, blk;
+    origin(item, o0, o1, o2, blk);
+    const int c0 = per_group ? 0 : blk, c1 = per_group ? b.ncomp : blk + 1;
+    // the first window of this item was copied into Cc by the previous item
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
 
     // D_d = max over the block's components of |undivided difference in d|
     // (valid where the difference's three points are in the window)
     for (int comp = c0; comp < c1; ++comp) {
-      __syncthreads();
-      load(comp);
+      if (comp != c0) {
+        __syncthreads();
+        load(Cc, o0, o1, o2, comp, false);
+      }
       __syncthreads();
 #pragma unroll
       for (int n = 0; n < NWIN; ++n) {
         const int e = tid + n * ENT;
         if (e >= EW3)
           break;
-        const double cx = fabs(undiv2(C[e - 1], C[e], C[e + 1]));
-        const double cy = fabs(undiv2(C[e - EW], C[e], C[e + EW]));
-        const double cz = fabs(undiv2(C[e - EW * EW], C[e], C[e + EW * EW]));
+        const double cx = fabs(undiv2(Cc[e - 1], Cc[e], Cc[e + 1]));
+        const double cy = fabs(undiv2(Cc[e - EW], Cc[e], Cc[e + EW]));
+        const double cz = fabs(undiv2(Cc[e - EW * EW], Cc[e], Cc[e + EW * EW]));
         if (comp == c0) {
           D0[e] = cx;
           D1[e] = cy;
@@ -209,11 +240,20 @@ __global__ void __launch_bounds__(ENT, 2)
       shz[q] = bz;
     }
 
+    // copy the first window of this CTA's next item into the other buffer
+    // while this one evaluates
+    if (item + (int)gridDim.x < nitems) {
+      int p0, p1, p2, pblk;
+      origin(item + gridDim.x, p0, p1, p2, pblk);
+      load(Cn, p0, p1, p2, per_group ? 0 : pblk, true);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+
     // evaluate the children of every cell, component by component
     for (int comp = c0; comp < c1; ++comp) {
       if (c1 - c0 > 1 || comp != c1 - 1) { // the window holds the last component loaded
         __syncthreads();
-        load(comp);
+        load(Cc, o0, o1, o2, comp, false);
         __syncthreads();
       }
       double *fb = b.fine ? b.fine + comp * b.fnp : nullptr;
@@ -243,7 +283,7 @@ __global__ void __launch_bounds__(ENT, 2)
           for (int g = 0; g < 3; ++g)
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-              const double *v = sh.c + base + EW * a + EW * EW * g;
+              const double *v = Cc + base + EW * a + EW * EW * g;
               X[a][g] = eno2_apply(wx, v[0], v[1], v[2]);
             }
 #pragma unroll
@@ -279,7 +319,11 @@ __global__ void __launch_bounds__(ENT, 2)
       }
     }
     __syncthreads(); // the next item reuses the shared arrays
+    double *const t_ = Cc;
+    Cc = Cn;
+    Cn = t_;
   }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
 bool g_eno_attr = false;
