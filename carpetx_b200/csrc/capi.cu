@@ -541,10 +541,13 @@ int cx_level_plan_execute(cx_level_plan_t p, cx_stream_t stream) {
       after_level = true;
     }
   }
-  for (int id : p->point_boxes)
-    if (int e = cuda_status(launch_point_box(p->boxes[id], p->per_group, nullptr, nullptr, s),
-                            "level launch (limited operators)"))
+  for (int id : p->point_boxes) {
+    if (int e = cuda_status(
+            launch_point_box(p->boxes[id], p->per_group, nullptr, nullptr, s, after_level),
+            "level launch (limited operators)"))
       return e;
+    after_level = true;
+  }
   return CX_OK;
 }
 

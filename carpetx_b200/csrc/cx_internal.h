@@ -71,14 +71,17 @@ int stream_level_grid(int group);
 // that it spreads over at least that many CTAs where it can.
 void stream_tiling(BoxDesc &b, int min_items);
 
+// after_level: as for launch_stream_level (the box's launch directly follows
+// another launch of the same level transfer on s); used by the ENO kernel.
 cudaError_t launch_point_box(const BoxDesc &b, int per_group,
                              signed char *shifts, unsigned char *fallback,
-                             cudaStream_t s);
+                             cudaStream_t s, bool after_level = false);
 // The per-coarse-cell ENO kernel takes operators whose three directions are
 // CC ENO 2 without an active linear fallback (launch_point_box forwards).
 bool eno_cell_applies(const BoxDesc &b, int per_group);
 cudaError_t launch_eno_cell_box(const BoxDesc &b, int per_group, signed char *shifts,
-                                unsigned char *fallback, cudaStream_t s);
+                                unsigned char *fallback, cudaStream_t s,
+                                bool after_level = false);
 cudaError_t launch_point_level(const BoxDesc *d_boxes, const TileRef *d_tiles,
                                int ntiles, int per_group, cudaStream_t s);
 

@@ -81,6 +81,10 @@ struct EnoTiling {
 __global__ void __launch_bounds__(ENT, 2)
     eno_cell_kernel(const __grid_constant__ BoxDesc b, const EnoTiling t, int per_group,
                     signed char *shifts, unsigned char *fallback) {
+  // the launches of a level's boxes after its first start in the previous
+  // launch's tail and wait for it at their end (programmatic dependent
+  // launch; no-ops without the launch attribute)
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   EnoShared &sh = *reinterpret_cast<EnoShared *>(smem_raw);
   // the window arrays as one run of doubles, guards included, for the
@@ -324,6 +328,7 @@ __global__ void __launch_bounds__(ENT, 2)
     Cn = t_;
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 bool g_eno_attr = false;
@@ -337,7 +342,7 @@ bool eno_cell_applies(const BoxDesc &b, int per_group) {
 }
 
 cudaError_t launch_eno_cell_box(const BoxDesc &b, int per_group, signed char *shifts,
-                                unsigned char *fallback, cudaStream_t s) {
+                                unsigned char *fallback, cudaStream_t s, bool after_level) {
   if (b.ncomp <= 0)
     return cudaSuccess;
   EnoTiling t;
@@ -364,9 +369,17 @@ cudaError_t launch_eno_cell_box(const BoxDesc &b, int per_group, signed char *sh
     g_eno_grid = sms * (per_sm > 0 ? per_sm : 1);
     g_eno_attr = true;
   }
-  const int grid = n < g_eno_grid ? (int)n : g_eno_grid;
-  eno_cell_kernel<<<grid, ENT, sizeof(EnoShared), s>>>(b, t, per_group, shifts, fallback);
-  return cudaGetLastError();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(n < g_eno_grid ? (unsigned)n : (unsigned)g_eno_grid);
+  cfg.blockDim = dim3(ENT);
+  cfg.dynamicSmemBytes = sizeof(EnoShared);
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = after_level ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, eno_cell_kernel, b, t, per_group, shifts, fallback);
 }
 
 } // namespace cxb

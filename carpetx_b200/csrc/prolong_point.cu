@@ -427,9 +427,9 @@ __global__ void __launch_bounds__(AT_NT)
 } // namespace
 
 cudaError_t launch_point_box(const BoxDesc &b, int per_group, signed char *shifts,
-                             unsigned char *fallback, cudaStream_t s) {
+                             unsigned char *fallback, cudaStream_t s, bool after_level) {
   if (eno_cell_applies(b, per_group)) // all directions ENO, no fallback
-    return launch_eno_cell_box(b, per_group, shifts, fallback, s);
+    return launch_eno_cell_box(b, per_group, shifts, fallback, s, after_level);
   const int64_t rnp = (int64_t)(b.rhi[0] - b.rlo[0] + 1) * (b.rhi[1] - b.rlo[1] + 1) *
                       (b.rhi[2] - b.rlo[2] + 1);
   if (rnp <= 0 || b.ncomp <= 0)
