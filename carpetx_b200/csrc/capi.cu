@@ -189,6 +189,7 @@ struct cx_level_plan {
   std::vector<int> point_boxes; // boxes handled by the pointwise kernel
   BoxDesc *d_boxes = nullptr;
   TileRef *d_tiles = nullptr;
+  int *d_counters = nullptr; // forward plans: one item counter per group
   int nsep_tiles = 0;
   // items of kernel group g: [group_off[g], group_off[g + 1]) of d_tiles
   int group_off[kStrGroups + 1] = {};
@@ -269,7 +270,9 @@ int cx_prolong_box_diag(cx_op_t op, const double *crse, const int crse_lo[3], co
   if (int e = check_device())
     return e;
   cudaStream_t s = (cudaStream_t)stream;
-  if (use_stream(op, per_group)) // one box per launch: spread it over the GPU
+  // one box per launch: spread it over the GPU (z chunks sized by the grid of
+  // the 256-thread variant, whichever CTA size the box then takes)
+  if (use_stream(op, per_group))
     stream_tiling(b, stream_level_grid(stream_group_of(b.kind[0], b.kind[1], b.kind[2])));
   if (use_stream(op, per_group) && !shifts && !fallback)
     return cuda_status(launch_stream_box(b, s), "prolongation launch");
@@ -356,7 +359,7 @@ int cx_level_plan_create(const cx_box_t *boxes, int nboxes, int per_group, cx_le
   // by z-window group (one kernel each), then by cost, largest first
   auto group_of = [&](const TileRef &t) {
     const BoxDesc &b = p->boxes[t.box];
-    return stream_group_of(b.kind[0], b.kind[1], b.kind[2]);
+    return stream_group_of(b.kind[0], b.kind[1], b.kind[2]) + (b.scta ? kStrKinds : 0);
   };
   std::stable_sort(keyed.begin(), keyed.end(),
                    [&](const std::pair<int, TileRef> &a, const std::pair<int, TileRef> &b) {
@@ -381,6 +384,8 @@ int cx_level_plan_create(const cx_box_t *boxes, int nboxes, int per_group, cx_le
     e = cudaMalloc(&p->d_boxes, sizeof(BoxDesc) * p->boxes.size());
   if (e == cudaSuccess && !tiles.empty())
     e = cudaMalloc(&p->d_tiles, sizeof(TileRef) * tiles.size());
+  if (e == cudaSuccess && !tiles.empty())
+    e = cudaMalloc(&p->d_counters, sizeof(int) * kStrGroups);
   if (e == cudaSuccess && !p->boxes.empty())
     e = cudaMemcpy(p->d_boxes, p->boxes.data(), sizeof(BoxDesc) * p->boxes.size(),
                    cudaMemcpyHostToDevice);
@@ -530,12 +535,20 @@ int cx_level_plan_execute(cx_level_plan_t p, cx_stream_t stream) {
     }
     return CX_OK;
   }
+  if (p->d_counters)
+    if (int e = cuda_status(cudaMemsetAsync(p->d_counters, 0, sizeof(int) * kStrGroups, s),
+                            "memset"))
+      return e;
+  // the 128-thread groups first: their few items then run beside the
+  // 256-thread groups instead of after them
   bool after_level = false;
-  for (int g = 0; g < kStrGroups; ++g) {
+  for (int i = 0; i < kStrGroups; ++i) {
+    const int g = (i + kStrKinds) % kStrGroups;
     const int n = p->group_off[g + 1] - p->group_off[g];
     if (n > 0) {
       if (int e = cuda_status(launch_stream_level(g, p->d_boxes, p->d_tiles + p->group_off[g], n,
-                                                  p->group_grid[g], s, after_level),
+                                                  p->group_grid[g], p->d_counters + g, s,
+                                                  after_level),
                               "level launch"))
         return e;
       after_level = true;
@@ -581,6 +594,7 @@ int cx_level_plan_destroy(cx_level_plan_t p) {
     return CX_OK;
   cudaFree(p->d_boxes);
   cudaFree(p->d_tiles);
+  cudaFree(p->d_counters);
   delete p;
   return CX_OK;
 }

@@ -7,9 +7,13 @@
 
 namespace cxb {
 
-// Streaming kernel: threads per CTA, column units per thread; at most
-// kStrPairRows pairs of fine y rows and kStrMaxWidth fine x per item.
+// Streaming kernel: threads per CTA (kStrThreadsSmall for the items of
+// boxes with at most kStrSmallUnits column units per x chunk), column units
+// per thread; at most kStrPairRows pairs of fine y rows and kStrMaxWidth fine
+// x per item.
 constexpr int kStrThreads = 256;
+constexpr int kStrThreadsSmall = 128;
+constexpr int kStrSmallUnits = 256;
 constexpr int kStrUnitsPerThread = 2;
 constexpr int kStrPairRows = 64;
 constexpr int kStrMaxWidth = 130;
@@ -36,6 +40,7 @@ struct BoxDesc {
   int xcw;            // streaming kernel: fine x per x chunk
   int npr;            // streaming kernel: pairs of fine y rows
   int upi;            // streaming kernel: units (columns) per item
+  int scta;           // streaming kernel: 1 = the 128-thread variant
   double *cbar;       // adjoint: coarse output (P^T fine)
   int at[3];          // adjoint: coarse tile extents in x, y; coarse z per item
   int ant[3];         // adjoint: tiles per direction
@@ -55,16 +60,20 @@ cudaError_t launch_stream_box(const BoxDesc &b, cudaStream_t s);
 int stream_pair_of(int kx, int ky, int kz);
 // Streaming-kernel instantiation serving an operator's kinds:
 // 8 x pair + (cx << 2 | cy << 1 | cz), c = 1 for a cell-centred direction;
-// -1 if none.
+// -1 if none.  A level's groups add kStrKinds for the 128-thread variant
+// (BoxDesc::scta).
 int stream_group_of(int kx, int ky, int kz);
-constexpr int kStrGroups = 136; // number of instantiations (8 x kStreamPairs)
+constexpr int kStrKinds = 136;            // instantiations per CTA size (8 x kStreamPairs)
+constexpr int kStrGroups = 2 * kStrKinds; // level groups: both CTA sizes
 // Level launch of the items of one instantiation; d_items holds only items
-// of boxes served by that group.  after_level: the launch directly follows
-// another level launch of the same transfer on s (boxes disjoint), and may
-// start while that one finishes (programmatic dependent launch).
+// of boxes served by that group, sorted by cost; d_counter: one int, zero
+// before the launch (the CTAs take items from it).  after_level: the launch
+// directly follows another level launch of the same transfer on s (boxes
+// disjoint), and may start while that one finishes (programmatic dependent
+// launch).
 cudaError_t launch_stream_level(int group, const BoxDesc *d_boxes,
                                 const TileRef *d_items, int nitems, int grid,
-                                cudaStream_t s, bool after_level);
+                                int *d_counter, cudaStream_t s, bool after_level);
 int stream_level_grid(int group);
 // Fills the streaming-kernel tiling of a box (tbase, ntile, zchunk, xcw,
 // npr, upi); min_items > 0 shortens the z chunks of a box launched alone so

@@ -34,6 +34,7 @@ constexpr int kMaxItems = CX_NOALLOC_MAX_ITEMS;
 struct WorkList {
   BoxDesc boxes[kMaxBoxes];
   TileRef items[kMaxItems];
+  int counters[kStrGroups]; // item counter per group, zeroed by every call
 };
 
 // The scratch: one work list per GPU (about 1.7 MB), shared by every call.
@@ -115,7 +116,7 @@ extern "C" int cx_level_execute_noalloc(const cx_box_t *boxes, int nboxes, int p
       if (point[id])
         continue;
       const BoxDesc &b = g_stage.boxes[id];
-      const int g = stream_group_of(b.kind[0], b.kind[1], b.kind[2]);
+      const int g = stream_group_of(b.kind[0], b.kind[1], b.kind[2]) + (b.scta ? kStrKinds : 0);
       for (int c = 0; c < b.ncomp; ++c)
         for (int tz = 0; tz < b.ntile[2]; ++tz)
           for (int tx = 0; tx < b.ntile[0]; ++tx) {
@@ -167,11 +168,13 @@ extern "C" int cx_level_execute_noalloc(const cx_box_t *boxes, int nboxes, int p
   if (e == cudaSuccess && nitems > 0)
     e = cudaMemcpyAsync(dev->items, g_stage.items, sizeof(TileRef) * nitems,
                         cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && nitems > 0)
+    e = cudaMemsetAsync(dev->counters, 0, sizeof(int) * kStrGroups, s);
   for (int g = 0; e == cudaSuccess && g < kStrGroups; ++g) {
     const int n = off[g + 1] - off[g];
     if (n > 0)
-      e = launch_stream_level(g, dev->boxes, dev->items + off[g], n, stream_level_grid(g), s,
-                              false);
+      e = launch_stream_level(g, dev->boxes, dev->items + off[g], n, stream_level_grid(g),
+                              dev->counters + g, s, false);
   }
   for (int id = 0; e == cudaSuccess && id < nb; ++id)
     if (point[id])

@@ -4,29 +4,37 @@
 
 namespace cxb {
 namespace stream {
-KernelFn kernel_part0(int group);
-KernelFn kernel_part1(int group);
-KernelFn kernel_part2(int group);
-KernelFn kernel_part3(int group);
-KernelFn kernel_part4(int group);
-KernelFn kernel_part5(int group);
-KernelFn kernel_part6(int group);
-KernelFn kernel_part7(int group);
+KernelFn kernel_part0(int group, bool small_cta);
+KernelFn kernel_part1(int group, bool small_cta);
+KernelFn kernel_part2(int group, bool small_cta);
+KernelFn kernel_part3(int group, bool small_cta);
+KernelFn kernel_part4(int group, bool small_cta);
+KernelFn kernel_part5(int group, bool small_cta);
+KernelFn kernel_part6(int group, bool small_cta);
+KernelFn kernel_part7(int group, bool small_cta);
 
 namespace {
 bool g_attr_set[kStrGroups] = {};
 
-// Kernel of a group; the first lookup allows its dynamic shared memory
-// (sizeof(Shared), which may exceed the 48 KB default).
+// Threads and dynamic shared memory of a level group's CTA size.
+int threads_of(int group) { return group >= kStrKinds ? small::NTS : big::NTS; }
+size_t smem_of(int group) {
+  return group >= kStrKinds ? sizeof(small::Shared) : sizeof(big::Shared);
+}
+
+// Kernel of a level group (instantiation + kStrKinds for the 128-thread
+// variant); the first lookup allows its dynamic shared memory, which may
+// exceed the 48 KB default.
 KernelFn kernel_for(int group) {
   if (group < 0 || group >= kStrGroups)
     return nullptr;
-  static KernelFn (*const parts[kStreamParts])(int) = {kernel_part0, kernel_part1, kernel_part2,
-                                                        kernel_part3, kernel_part4, kernel_part5,
-                                                        kernel_part6, kernel_part7};
-  KernelFn k = parts[group % kStreamParts](group);
+  static KernelFn (*const parts[kStreamParts])(int, bool) = {
+      kernel_part0, kernel_part1, kernel_part2, kernel_part3,
+      kernel_part4, kernel_part5, kernel_part6, kernel_part7};
+  const int kind = group % kStrKinds;
+  KernelFn k = parts[kind % kStreamParts](kind, group >= kStrKinds);
   if (k && !g_attr_set[group]) {
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Shared));
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_of(group));
     g_attr_set[group] = true;
   }
   return k;
@@ -82,7 +90,8 @@ void stream_tiling(BoxDesc &b, int min_items) {
   using namespace stream;
   for (int d = 0; d < 3; ++d)
     b.tbase[d] = b.rlo[d] & ~1;
-  // x chunks: the whole width up to WFMAX, else near-equal even chunks
+  // x chunks: the whole width up to kStrMaxWidth, else near-equal even chunks
+  constexpr int WFMAX = kStrMaxWidth, PRMAX = kStrPairRows;
   const int Wt = b.rhi[0] - b.tbase[0] + 1;
   if (Wt <= WFMAX) {
     b.xcw = Wt;
@@ -95,7 +104,11 @@ void stream_tiling(BoxDesc &b, int min_items) {
     b.ntile[0] = (Wt + w - 1) / w;
   }
   b.npr = (b.rhi[1] - b.tbase[1]) / 2 + 1;
-  b.upi = NU < PRMAX * b.xcw ? NU : PRMAX * b.xcw;
+  // boxes with at most kStrSmallUnits column units per x chunk run on the
+  // 128-thread variant (one item of 256 unit slots instead of 512)
+  b.scta = b.npr * b.xcw <= kStrSmallUnits ? 1 : 0;
+  const int nu = b.scta ? small::NU : big::NU;
+  b.upi = nu < PRMAX * b.xcw ? nu : PRMAX * b.xcw;
   b.ntile[1] = (b.npr * b.xcw + b.upi - 1) / b.upi;
   // fine z per item: whole columns up to 128 fine points, else near-equal
   // even chunks of at most 128 (the z halo and the pipeline start cost extra
@@ -120,7 +133,7 @@ int stream_level_grid(int group) {
     return 0;
   if (!g_grid[group]) {
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NTS, sizeof(Shared));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads_of(group), smem_of(group));
     g_grid[group] = sms() * (per_sm > 0 ? per_sm : 1);
   }
   return g_grid[group];
@@ -133,18 +146,22 @@ cudaError_t launch_stream_box(const BoxDesc &b, cudaStream_t s) {
     return cudaSuccess;
   if (n64 > INT32_MAX)
     return cudaErrorInvalidValue;
-  const int group = stream_group_of(b.kind[0], b.kind[1], b.kind[2]);
+  const int kind = stream_group_of(b.kind[0], b.kind[1], b.kind[2]);
+  if (kind < 0)
+    return cudaErrorInvalidValue;
+  const int group = kind + (b.scta ? kStrKinds : 0);
   KernelFn k = kernel_for(group);
   if (!k)
     return cudaErrorInvalidValue;
   const int n = (int)n64;
   const int cap = stream_level_grid(group);
-  k<<<n < cap ? n : cap, NTS, sizeof(Shared), s>>>(b, nullptr, nullptr, n);
+  k<<<n < cap ? n : cap, threads_of(group), smem_of(group), s>>>(b, nullptr, nullptr, n, nullptr);
   return cudaGetLastError();
 }
 
 cudaError_t launch_stream_level(int group, const BoxDesc *d_boxes, const TileRef *d_items,
-                                int nitems, int grid, cudaStream_t s, bool after_level) {
+                                int nitems, int grid, int *d_counter, cudaStream_t s,
+                                bool after_level) {
   using namespace stream;
   if (nitems <= 0)
     return cudaSuccess;
@@ -154,15 +171,15 @@ cudaError_t launch_stream_level(int group, const BoxDesc *d_boxes, const TileRef
   BoxDesc unused{};
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid < nitems ? grid : nitems);
-  cfg.blockDim = dim3(NTS);
-  cfg.dynamicSmemBytes = sizeof(Shared);
+  cfg.blockDim = dim3(threads_of(group));
+  cfg.dynamicSmemBytes = smem_of(group);
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = after_level ? 1 : 0;
-  return cudaLaunchKernelEx(&cfg, k, unused, d_boxes, d_items, nitems);
+  return cudaLaunchKernelEx(&cfg, k, unused, d_boxes, d_items, nitems, d_counter);
 }
 
 } // namespace cxb

@@ -1,17 +1,17 @@
 // Streaming-kernel instantiations, part 0 of kStreamParts: the kernels whose
 // centring (cx << 2 | cy << 1 | cz) is 0, one per stencil pair of
-// stream_pairs.h; split only to compile in parallel.
+// stream_pairs.h and CTA size; split only to compile in parallel.
 #include "stream_kernel.cuh"
 #include "stream_pairs.h"
 
 namespace cxb {
 namespace stream {
 
-KernelFn kernel_part0(int group) {
+KernelFn kernel_part0(int group, bool small_cta) {
   switch (group) {
 #define CXB_PAIR_CASE(I, V, C, KVI, KCI)                                       \
   case kStreamParts * I + 0:                                                   \
-    return stream_kernel<V, C, 0>;
+    return small_cta ? small::stream_kernel<V, C, 0> : big::stream_kernel<V, C, 0>;
     CXB_STREAM_PAIRS(CXB_PAIR_CASE)
 #undef CXB_PAIR_CASE
   default:
