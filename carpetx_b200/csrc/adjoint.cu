@@ -134,12 +134,14 @@ cudaError_t launch_prolong_adjoint_box(const BoxDesc &b0, int per_group, double 
   if (n64 > INT32_MAX)
     return cudaErrorInvalidValue;
   const int n = (int)n64;
-  k<<<n < g_adj_grid[group] ? n : g_adj_grid[group], NT, smem, s>>>(b, nullptr, nullptr, n);
+  k<<<n < g_adj_grid[group] ? n : g_adj_grid[group], NT, smem, s>>>(b, nullptr, nullptr, n,
+                                                                     nullptr);
   return cudaGetLastError();
 }
 
 cudaError_t launch_adjoint_level(int group, const BoxDesc *d_boxes, const TileRef *d_items,
-                                 int nitems, int grid, cudaStream_t s, bool after_level) {
+                                 int nitems, int grid, int *d_counter, cudaStream_t s,
+                                 bool after_level) {
   if (nitems <= 0)
     return cudaSuccess;
   size_t smem = 0;
@@ -157,7 +159,7 @@ cudaError_t launch_adjoint_level(int group, const BoxDesc *d_boxes, const TileRe
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = after_level ? 1 : 0;
-  return cudaLaunchKernelEx(&cfg, k, unused, d_boxes, d_items, nitems);
+  return cudaLaunchKernelEx(&cfg, k, unused, d_boxes, d_items, nitems, d_counter);
 }
 
 } // namespace cxb

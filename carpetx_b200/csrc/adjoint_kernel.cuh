@@ -474,16 +474,17 @@ static_assert(BOX_WORDS <= NT, "one thread per descriptor word");
 
 // Box mode (items == nullptr): the items of box b strided over the grid.
 // Level mode: items of a device work list (sorted by cost, the tiles of a box
-// together) strided over persistent CTAs.  One instantiation per stencil pair
+// together) taken by persistent CTAs from a counter.  One instantiation per stencil pair
 // and centring CM = (cx << 2) | (cy << 1) | cz (1: cell centred).
 template <class KV, class KC, int CM>
 __global__ void __launch_bounds__(NT, AdjPair<KV, KC>::OCC)
     adjoint_kernel(const __grid_constant__ BoxDesc b, const BoxDesc *__restrict__ boxes,
-                   const TileRef *__restrict__ items, int nitems) {
+                   const TileRef *__restrict__ items, int nitems, int *__restrict__ counter) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ BoxDesc box_s;
   __shared__ uint64_t mbar[NBUF];
   __shared__ int s_fail;
+  __shared__ int s_take;
   double *fbuf = reinterpret_cast<double *>(smem_raw);
   double *gbuf = fbuf + NBUF * AdjPair<KV, KC>::FP;
   // level launches after the first of a plan start in the previous one's
@@ -498,7 +499,9 @@ __global__ void __launch_bounds__(NT, AdjPair<KV, KC>::OCC)
   }
   __syncthreads();
   uint32_t phase = 0; // completed-phase parity per buffer
-  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+  // level mode: after item blockIdx.x, a CTA takes the next untaken item of
+  // the list (sorted by cost) from the launch's counter (zero before it)
+  for (int item = blockIdx.x; item < nitems;) {
     const BoxDesc *bp = &b;
     int xt, yt, zt, comp;
     if (items) {
@@ -528,12 +531,20 @@ __global__ void __launch_bounds__(NT, AdjPair<KV, KC>::OCC)
         adj_item<KV, KC, KX, KY, KZ>(fbuf, gbuf, mbar, &s_fail, phase, *bp, xt, yt, zt, comp);
     if (!ok)
       break;
-    // adj_item ends with a barrier: box_s may be overwritten
+    // adj_item ends with a barrier: box_s and s_take may be overwritten
+    if (items) {
+      if (threadIdx.x == 0)
+        s_take = gridDim.x + atomicAdd(counter, 1);
+      __syncthreads();
+      item = s_take;
+    } else {
+      item += gridDim.x;
+    }
   }
   asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
-using AdjFn = void (*)(const BoxDesc, const BoxDesc *, const TileRef *, int);
+using AdjFn = void (*)(const BoxDesc, const BoxDesc *, const TileRef *, int, int *);
 
 // Kernel and shared-memory size of a pair and centring (nullptr for the
 // nonlinear pairs).

@@ -189,7 +189,7 @@ struct cx_level_plan {
   std::vector<int> point_boxes; // boxes handled by the pointwise kernel
   BoxDesc *d_boxes = nullptr;
   TileRef *d_tiles = nullptr;
-  int *d_counters = nullptr; // forward plans: one item counter per group
+  int *d_counters = nullptr; // one item counter per group
   int nsep_tiles = 0;
   // items of kernel group g: [group_off[g], group_off[g + 1]) of d_tiles
   int group_off[kStrGroups + 1] = {};
@@ -497,6 +497,8 @@ int cx_level_plan_create_adjoint(const cx_box_t *boxes, int nboxes, int per_grou
     e = cudaMalloc(&p->d_boxes, sizeof(BoxDesc) * p->boxes.size());
   if (e == cudaSuccess && !tiles.empty())
     e = cudaMalloc(&p->d_tiles, sizeof(TileRef) * tiles.size());
+  if (e == cudaSuccess && !tiles.empty())
+    e = cudaMalloc(&p->d_counters, sizeof(int) * kStrGroups);
   if (e == cudaSuccess && !p->boxes.empty())
     e = cudaMemcpy(p->d_boxes, p->boxes.data(), sizeof(BoxDesc) * p->boxes.size(),
                    cudaMemcpyHostToDevice);
@@ -522,12 +524,17 @@ int cx_level_plan_execute(cx_level_plan_t p, cx_stream_t stream) {
     for (auto &z : p->zero_boxes)
       if (int e = cuda_status(cudaMemsetAsync(z.first, 0, z.second, s), "memset"))
         return e;
+    if (p->d_counters)
+      if (int e = cuda_status(cudaMemsetAsync(p->d_counters, 0, sizeof(int) * kStrGroups, s),
+                              "memset"))
+        return e;
     bool after_level = false;
     for (int g = 0; g < kStrGroups; ++g) {
       const int n = p->group_off[g + 1] - p->group_off[g];
       if (n > 0) {
         if (int e = cuda_status(launch_adjoint_level(g, p->d_boxes, p->d_tiles + p->group_off[g],
-                                                     n, p->group_grid[g], s, after_level),
+                                                     n, p->group_grid[g], p->d_counters + g, s,
+                                                     after_level),
                                 "adjoint level launch"))
           return e;
         after_level = true;

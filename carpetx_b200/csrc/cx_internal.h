@@ -125,9 +125,9 @@ int adjoint_level_grid(int group);
 // 1 if a bounded wait of the adjoint kernels gave up since the last call
 // (and clears the flag), 0 if not, -1 if the flag could not be read.
 int adjoint_take_timeout();
-// after_level: as for launch_stream_level.
+// d_counter, after_level: as for launch_stream_level.
 cudaError_t launch_adjoint_level(int group, const BoxDesc *d_boxes,
                                  const TileRef *d_items, int nitems, int grid,
-                                 cudaStream_t s, bool after_level);
+                                 int *d_counter, cudaStream_t s, bool after_level);
 
 } // namespace cxb
