@@ -19,7 +19,8 @@ One step = prolongation of every box and component of the level.  Reported:
              reference's launch granularity), our kernel
   e2e        through the C ABI with host buffers: pinned host -> device copy
              of the coarse data, the level transfer, device -> host copy of
-             the fine data, every step
+             the fine data, every step; the level in 8 box batches (one plan
+             each) so that copies in, transfers and copies out overlap
   roofline   algorithmic bytes 8 (|CoarseBox(region)| + |region|) per box and
              component over the kernel time, against the measured HBM copy
              bandwidth
@@ -54,6 +55,7 @@ sys.path.insert(0, ROOT)
 METRIC = "FP64 fine points/s, batched persistent level prolongation"
 UNIT = "fine points/s"
 L2_BYTES = 126 * 1024 * 1024
+E2E_BATCHES = 8  # box batches of the end-to-end leg's copy/transfer pipeline
 # ncu DRAM bytes per fine point of the level512 workload (the four kernels of
 # a step, 2-component capture: 282.5 MB read + 1145.8 MB written for
 # 172,696,778 fine points; ncu flushes the L2 between launches, so the fine
@@ -533,23 +535,62 @@ def main():
         ms_pb = max_over_ranks(e0.elapsed_time(e1)) / args.per_box_steps
         per_box_value = total_fine / (ms_pb / 1e3)
 
-    # end to end through the C ABI with host buffers
+    # end to end through the C ABI with host buffers: every step copies all
+    # coarse data in from pinned host memory and all fine data out.  The
+    # level is split into E2E_BATCHES batches of consecutive boxes, one plan
+    # each, pipelined over three streams: batch k's copy in, transfer and
+    # copy out wait for each other, and the copy in (copy out) of a batch
+    # waits for the previous step's transfer (copy out) of that batch, whose
+    # buffers it overwrites.  Copies in and out then run at the same time on
+    # the two copy directions, beside the transfers.
     ms_e2e, e2e_value = None, None
     if args.e2e_steps > 0:
         h_crse = torch.empty(ctot, dtype=torch.float64, pin_memory=True)
         h_fine = torch.empty(ftot, dtype=torch.float64, pin_memory=True)
         h_crse.copy_(crse.cpu())
+        nb = len(lb)
+        cuts = sorted({round(i * nb / E2E_BATCHES) for i in range(E2E_BATCHES + 1)})
+        coff_all, foff_all = coff + [ctot], foff + [ftot]
+        batches = [(cb.LevelPlan(lb[a:z]), coff_all[a], coff_all[z], foff_all[a], foff_all[z])
+                   for a, z in zip(cuts[:-1], cuts[1:]) if z > a]
+        s_in, s_out = torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev)
+        done_x = [None] * len(batches)  # previous step's transfer of batch k
+        done_o = [None] * len(batches)  # previous step's copy out of batch k
+
+        def e2e_step():
+            for k, (bp, c0, c1, f0, f1) in enumerate(batches):
+                ev_in, ev_x, ev_o = torch.cuda.Event(), torch.cuda.Event(), torch.cuda.Event()
+                with torch.cuda.stream(s_in):
+                    if done_x[k] is not None:
+                        s_in.wait_event(done_x[k])
+                    crse[c0:c1].copy_(h_crse[c0:c1], non_blocking=True)
+                    ev_in.record(s_in)
+                stream.wait_event(ev_in)
+                if done_o[k] is not None:
+                    stream.wait_event(done_o[k])
+                bp.execute(stream)
+                ev_x.record(stream)
+                with torch.cuda.stream(s_out):
+                    s_out.wait_event(ev_x)
+                    h_fine[f0:f1].copy_(fine[f0:f1], non_blocking=True)
+                    ev_o.record(s_out)
+                done_x[k], done_o[k] = ev_x, ev_o
+
+        e2e_step()
+        torch.cuda.synchronize()
         barrier()
         e0.record(stream)
-        with torch.cuda.stream(stream):
-            for _ in range(args.e2e_steps):
-                crse.copy_(h_crse, non_blocking=True)
-                plan.execute(stream)
-                h_fine.copy_(fine, non_blocking=True)
+        s_in.wait_stream(stream)
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        stream.wait_stream(s_in)
+        stream.wait_stream(s_out)
         e1.record(stream)
         barrier()
         ms_e2e = max_over_ranks(e0.elapsed_time(e1)) / args.e2e_steps
         e2e_value = total_fine / (ms_e2e / 1e3)
+        for bp, *_ in batches:
+            bp.close()
 
     adjoint = adjoint_leg(args, cb, torch, dev, max_over_ranks, barrier) if args.adjoint_steps > 0 \
         else None
