@@ -56,11 +56,11 @@ METRIC = "FP64 fine points/s, batched persistent level prolongation"
 UNIT = "fine points/s"
 L2_BYTES = 126 * 1024 * 1024
 E2E_BATCHES = 8  # box batches of the end-to-end leg's copy/transfer pipeline
-# ncu DRAM bytes per fine point of the level512 workload (the four kernels of
-# a step, 2-component capture: 282.5 MB read + 1145.8 MB written for
+# ncu DRAM bytes per fine point of the level512 workload (the eight kernels
+# of a step, 2-component capture: 283.2 MB read + 1138.3 MB written for
 # 172,696,778 fine points; ncu flushes the L2 between launches, so the fine
 # lines still dirty in the L2 when a launch ends are written back outside it)
-TRAFFIC_PER_FINE_POINT = 1428.28e6 / 172696778
+TRAFFIC_PER_FINE_POINT = 1421.55e6 / 172696778
 
 
 def parse():
