@@ -276,33 +276,41 @@ __global__ void __launch_bounds__(ENT, 2)
           eno2_coeffs(shy[q], o, wy[o]);
           eno2_coeffs(shz[q], o, wz[o]);
         }
-        // x lines at y = cj + shy - 1 + a, z = ck + shz - 1 + g
+        // x lines at y = cj + shy - 1 + a, z = ck + shz - 1 + g: each line's
+        // three points are read once for both fine x offsets
         const int base = cell[q] + (shx[q] - 1) + EW * (shy[q] - 1) + EW * EW * (shz[q] - 1);
-#pragma unroll 1
-        for (int ox = 0; ox < 2; ++ox) {
-          double wx[3];
-          eno2_coeffs(shx[q], ox, wx);
-          double X[3][3];
+        double wx[2][3];
 #pragma unroll
-          for (int g = 0; g < 3; ++g)
+        for (int o = 0; o < 2; ++o)
+          eno2_coeffs(shx[q], o, wx[o]);
+        double Y[2][2][3]; // [ox][oy][g]
 #pragma unroll
-            for (int a = 0; a < 3; ++a) {
-              const double *v = Cc + base + EW * a + EW * EW * g;
-              X[a][g] = eno2_apply(wx, v[0], v[1], v[2]);
-            }
+        for (int g = 0; g < 3; ++g) {
+          double X[2][3]; // [ox][a]
 #pragma unroll
-          for (int oy = 0; oy < 2; ++oy) {
-            double Y[3];
+          for (int a = 0; a < 3; ++a) {
+            const double *v = Cc + base + EW * a + EW * EW * g;
+            const double v0 = v[0], v1 = v[1], v2 = v[2];
+            X[0][a] = eno2_apply(wx[0], v0, v1, v2);
+            X[1][a] = eno2_apply(wx[1], v0, v1, v2);
+          }
 #pragma unroll
-            for (int g = 0; g < 3; ++g)
-              Y[g] = eno2_apply(wy[oy], X[0][g], X[1][g], X[2][g]);
+          for (int ox = 0; ox < 2; ++ox)
+#pragma unroll
+            for (int oy = 0; oy < 2; ++oy)
+              Y[ox][oy][g] = eno2_apply(wy[oy], X[ox][0], X[ox][1], X[ox][2]);
+        }
+#pragma unroll
+        for (int ox = 0; ox < 2; ++ox)
+#pragma unroll
+          for (int oy = 0; oy < 2; ++oy)
 #pragma unroll
             for (int oz = 0; oz < 2; ++oz) {
               const int fx = f0x + ox, fy = f0y + oy, fz = f0z + oz;
               if (fx < b.rlo[0] || fx > b.rhi[0] || fy < b.rlo[1] || fy > b.rhi[1] ||
                   fz < b.rlo[2] || fz > b.rhi[2])
                 continue;
-              const double r = eno2_apply(wz[oz], Y[0], Y[1], Y[2]);
+              const double r = eno2_apply(wz[oz], Y[ox][oy][0], Y[ox][oy][1], Y[ox][oy][2]);
               if (fb) // null: decisions only (the adjoint's decision pass)
                 fb[(fx - b.flo[0]) + (int64_t)b.fnx * (fy - b.flo[1]) + fplane * (fz - b.flo[2])] = r;
               if (comp == c0 && (shifts || fallback)) {
@@ -318,8 +326,6 @@ __global__ void __launch_bounds__(ENT, 2)
                   fallback[blk * rnp + ridx] = 0;
               }
             }
-          }
-        }
       }
     }
     __syncthreads(); // the next item reuses the shared arrays
