@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(ENT, 2)
       const int ci = u % ET, cj = (u / ET) % ET, ck = u / (ET * ET);
       cell[q] = widx(ci + 2, cj + 2, ck + 2);
       double min_dd = __longlong_as_double(0x7ff0000000000000LL); // +inf
-      int bx = 0, by = 0, bz = 0;
+      int best = 13; // candidate (si + 1) + 3 (sj + 1) + 9 (sk + 1); 13 = no shift
 #pragma unroll
       for (int sk = -1; sk <= 1; ++sk)
 #pragma unroll
@@ -231,17 +231,16 @@ __global__ void __launch_bounds__(ENT, 2)
             // for |s|_1 <= 3, a constant per candidate
             const int n1 = (si != 0) + (sj != 0) + (sk != 0);
             const double pen = 1.0 + 0x1p-26 * n1;
-            const double dd = fmul(pen, sh.m[cell[q] + si + EW * sj + EW * EW * sk]);
+            const double mv = sh.m[cell[q] + si + EW * sj + EW * EW * sk];
+            const double dd = n1 == 0 ? mv : fmul(pen, mv); // 1 * m is exact
             if (dd < min_dd) {
               min_dd = dd;
-              bx = si;
-              by = sj;
-              bz = sk;
+              best = (si + 1) + 3 * (sj + 1) + 9 * (sk + 1);
             }
           }
-      shx[q] = bx;
-      shy[q] = by;
-      shz[q] = bz;
+      shx[q] = best % 3 - 1;
+      shy[q] = (best / 3) % 3 - 1;
+      shz[q] = best / 9 - 1;
     }
 
     // copy the first window of this CTA's next item into the other buffer
