@@ -616,8 +616,10 @@ def main():
                        boxes_total=len(all_boxes), boxes_this_rank=len(boxes),
                        parallelism=f"weak: one level of {len(all_boxes)} boxes, knapsack-"
                                    f"distributed over {world} rank(s), no data-path collective",
-                       launch="one persistent kernel per step, CUDA graph replay"),
-        "gpu_launches": args.steps,
+                       launch=f"{st['launches']} persistent launches per step (one per kernel "
+                              "instantiation and CTA size present), each after the first a "
+                              "programmatic dependent launch; CUDA graph replay"),
+        "gpu_launches": args.steps * st["launches"],
         "per_box": {"value": per_box_value, "unit": UNIT, "ms_per_step": ms_pb,
                     "launches_per_step": len(calls),
                     "batched_speedup": value / per_box_value if per_box_value else None},

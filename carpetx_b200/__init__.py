@@ -78,6 +78,7 @@ def lib():
         L.cx_level_plan_stats.argtypes = [_VP, ctypes.POINTER(ctypes.c_int64),
                                           ctypes.POINTER(ctypes.c_int64),
                                           ctypes.POINTER(ctypes.c_int64)]
+        L.cx_level_plan_launches.argtypes = [_VP, ctypes.POINTER(_I)]
         L.cx_level_plan_destroy.argtypes = [_VP]
         L.cx_restrict_box.argtypes = [_I, _VP, _I3, _I3, _VP, _I3, _I3, _I3, _I3, _I, _VP]
         L.cx_restrict_adjoint_box.argtypes = [_I, _VP, _I3, _I3, _VP, _I3, _I3, _I3, _I3, _I, _VP]
@@ -225,7 +226,9 @@ class LevelPlan:
         a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         _check(lib().cx_level_plan_stats(self.handle, ctypes.byref(a), ctypes.byref(b),
                                          ctypes.byref(c)))
-        return {"tiles": a.value, "fine_points": b.value, "bytes": c.value}
+        n = ctypes.c_int()
+        _check(lib().cx_level_plan_launches(self.handle, ctypes.byref(n)))
+        return {"tiles": a.value, "fine_points": b.value, "bytes": c.value, "launches": n.value}
 
     def close(self):
         if self.handle:

@@ -596,6 +596,18 @@ int cx_level_plan_stats(cx_level_plan_t p, int64_t *ntiles, int64_t *nfine, int6
   return CX_OK;
 }
 
+int cx_level_plan_launches(cx_level_plan_t p, int *nlaunches) {
+  if (!p || !nlaunches)
+    return fail(CX_EINVAL, "invalid argument");
+  int n = 0;
+  for (int g = 0; g < kStrGroups; ++g)
+    n += p->group_off[g + 1] > p->group_off[g];
+  if (!p->adjoint)
+    n += (int)p->point_boxes.size();
+  *nlaunches = n;
+  return CX_OK;
+}
+
 int cx_level_plan_destroy(cx_level_plan_t p) {
   if (!p)
     return CX_OK;

@@ -145,6 +145,10 @@ int cx_level_plan_execute(cx_level_plan_t plan, cx_stream_t stream);
 /* Number of tiles and fine points (summed over components) in the plan. */
 int cx_level_plan_stats(cx_level_plan_t plan, int64_t *ntiles,
                         int64_t *nfine_points, int64_t *algorithmic_bytes);
+/* Kernel launches one execution enqueues: one per kernel instantiation
+ * present, plus one per box of the limited operators (besides the memset of
+ * the plan's item counters). */
+int cx_level_plan_launches(cx_level_plan_t plan, int *nlaunches);
 /* Frees the plan; the caller ensures no execution is still in flight. */
 int cx_level_plan_destroy(cx_level_plan_t plan);
 /* A level plan for the adjoint: executing it overwrites every box's crse
