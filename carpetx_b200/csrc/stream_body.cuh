@@ -95,8 +95,8 @@ struct Item {
   int c_first, c_last; // coarse planes streamed
   int pxw;             // row pitch of the x-pass result
   // this thread's units (tid and tid + NTS of the block): y window start in
-  // xs (-1: inactive unit); address of (fx, fy0) at fz = 0 (fy0 + 1 is fnx
-  // further); colmask bit j: fy0 + j inside the region
+  // xs (0 for a unit without a column); address of (fx, fy0) at fz = 0
+  // (fy0 + 1 is fnx further); colmask bit j: fy0 + j inside the region
   int ysrc[UPT];
   double *col[UPT];
   int colmask[UPT];
@@ -182,11 +182,12 @@ __device__ __forceinline__ void stream_item(Shared &sh, const Item &it) {
       __syncthreads();
       // ring slot ph takes plane c; logical position i (0 oldest) is slot
       // (ph + 1 + i) % L
+      // (units without a column read a valid part of xs and are never
+      // stored: no branch, so the compiler can interleave both units' work)
 #pragma unroll
       for (int q = 0; q < UPT; ++q) {
-        double y[FYT] = {0.0, 0.0};
-        if (it.ysrc[q] >= 0)
-          ypass<KY>(sh.xs + it.ysrc[q], it.pxw, y);
+        double y[FYT];
+        ypass<KY>(sh.xs + it.ysrc[q], it.pxw, y);
 #pragma unroll
         for (int j = 0; j < FYT; ++j)
           ring[ph][q][j] = y[j];
@@ -195,9 +196,10 @@ __device__ __forceinline__ void stream_item(Shared &sh, const Item &it) {
         const int cc = c - ZHI; // coarse centre whose stencil is complete
 #pragma unroll
         for (int off = 0; off < 2; ++off) {
+          // both offsets are evaluated; a fine z outside the chunk (its first
+          // or last plane) is only not stored
           const int fz = 2 * cc + off;
-          if (fz < it.zlo || fz > it.zhi)
-            continue;
+          const bool zin = fz >= it.zlo && fz <= it.zhi;
 #pragma unroll
           for (int q = 0; q < UPT; ++q)
 #pragma unroll
@@ -207,7 +209,7 @@ __device__ __forceinline__ void stream_item(Shared &sh, const Item &it) {
               for (int i = 0; i < L; ++i)
                 v[i] = ring[(ph + 1 + i) % L][q][j];
               const double r = off ? KZ::template ap<1>(v - ZLO) : KZ::template ap<0>(v - ZLO);
-              if (it.colmask[q] & (1 << j))
+              if (zin && (it.colmask[q] & (1 << j)))
                 __stcs(it.col[q] + j * it.fnx + (int64_t)fz * it.fplane, r);
             }
         }
@@ -261,7 +263,7 @@ __device__ __forceinline__ bool make_item(const BoxDesc &b, int xchunk, int ublo
   for (int q = 0; q < UPT; ++q) {
     const int u = u0 + (int)threadIdx.x + q * NTS;
     it.colmask[q] = 0;
-    it.ysrc[q] = -1;
+    it.ysrc[q] = 0; // no column: any in-bounds window of xs
     it.col[q] = b.fine;
     if (u < uend) {
       const int pr = u / W, fxl = u - pr * W;
