@@ -40,16 +40,18 @@ namespace cxb {
 namespace stream {
 
 namespace big {
-#define CXS_NTS 256
+#define CXS_NTS kStrThreads
 #include "stream_body.cuh"
 #undef CXS_NTS
 } // namespace big
 
 namespace small {
-#define CXS_NTS 128
+#define CXS_NTS kStrThreadsSmall
 #include "stream_body.cuh"
 #undef CXS_NTS
 } // namespace small
+
+static_assert(small::NU == kStrSmallUnits, "the small variant holds a small box's units");
 
 using KernelFn = void (*)(const BoxDesc, const BoxDesc *, const TileRef *, int, int *);
 
