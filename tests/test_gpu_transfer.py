@@ -122,6 +122,64 @@ def test_gpu_level_plan_matches_per_box(dev, cx):
     plan.close()
 
 
+def test_gpu_level_plans_pipelined_from_host(dev, cx):
+    """The host-resident pattern of the bench's end-to-end leg: a level split
+    into batches of boxes, one plan each, with copy in, transfer and copy out
+    on three streams over two steps (the second step's copies in overwrite
+    buffers the first step's transfers read).  Also: a plan's launch count is
+    one per kernel instantiation and CTA size present."""
+    rng = np.random.default_rng(12)
+    boxes = mixed_level(rng, 18, 2, smin=3, smax=24)
+    csz = [b["crse_np"].size for b in boxes]
+    fsz = [2 * int(np.prod(box_shape(b["fine_lo"], b["fine_hi"]))) for b in boxes]
+    coff, foff = np.concatenate([[0], np.cumsum(csz)]), np.concatenate([[0], np.cumsum(fsz)])
+    h_crse = torch.empty(int(coff[-1]), dtype=torch.float64, pin_memory=True)
+    h_fine = torch.full((int(foff[-1]),), np.nan, dtype=torch.float64, pin_memory=True)
+    crse = torch.empty(int(coff[-1]), dtype=torch.float64, device="cuda")
+    fine = torch.full((int(foff[-1]),), np.nan, dtype=torch.float64, device="cuda")
+    for b, c0, f0 in zip(boxes, coff, foff):
+        h_crse[c0:c0 + b["crse_np"].size] = torch.from_numpy(b["crse_np"].ravel())
+        b["crse"] = crse[c0:c0 + b["crse_np"].size].view(b["crse_np"].shape)
+        b["fine"] = fine[f0:f0 + 2 * int(np.prod(box_shape(b["fine_lo"], b["fine_hi"])))].view(
+            (2,) + box_shape(b["fine_lo"], b["fine_hi"]))
+    cuts = [0, 5, 11, 18]
+    plans = [cb.LevelPlan(boxes[a:z]) for a, z in zip(cuts[:-1], cuts[1:])]
+    for pl, a, z in zip(plans, cuts[:-1], cuts[1:]):
+        kinds = {(b["typ"], b["it"]) for b in boxes[a:z]}
+        assert 1 <= pl.stats()["launches"] <= 2 * len(kinds)
+    s_in, s_x, s_out = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+    done_x, done_o = [None] * 3, [None] * 3
+    torch.cuda.synchronize()
+    for step in range(2):
+        for k, (a, z) in enumerate(zip(cuts[:-1], cuts[1:])):
+            ev_in, ev_x, ev_o = torch.cuda.Event(), torch.cuda.Event(), torch.cuda.Event()
+            with torch.cuda.stream(s_in):
+                if done_x[k] is not None:
+                    s_in.wait_event(done_x[k])
+                crse[coff[a]:coff[z]].copy_(h_crse[coff[a]:coff[z]], non_blocking=True)
+                ev_in.record(s_in)
+            s_x.wait_event(ev_in)
+            if done_o[k] is not None:
+                s_x.wait_event(done_o[k])
+            plans[k].execute(s_x)
+            ev_x.record(s_x)
+            with torch.cuda.stream(s_out):
+                s_out.wait_event(ev_x)
+                h_fine[foff[a]:foff[z]].copy_(fine[foff[a]:foff[z]], non_blocking=True)
+                ev_o.record(s_out)
+            done_x[k], done_o[k] = ev_x, ev_o
+    torch.cuda.synchronize()
+    for b, f0 in zip(boxes, foff):
+        n = 2 * int(np.prod(box_shape(b["fine_lo"], b["fine_hi"])))
+        want = np.full((2,) + box_shape(b["fine_lo"], b["fine_hi"]), np.nan)
+        cx.prolong(b["typ"], b["order"], b["it"], 0, b["crse_np"], b["crse_lo"], b["crse_hi"],
+                   want, b["fine_lo"], b["fine_hi"], b["reg_lo"], b["reg_hi"], 2)
+        assert_bitwise(h_fine[f0:f0 + n].numpy().reshape(want.shape), want,
+                       f"pipelined {b['typ']} it{b['it']}")
+    for pl in plans:
+        pl.close()
+
+
 def test_gpu_level_plan_limited_and_empty(dev, cx):
     """A level mixing separable and limited (ENO, fallback) boxes and an empty
     region."""
