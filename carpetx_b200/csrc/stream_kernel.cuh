@@ -31,6 +31,12 @@
 // call_stencil_3d (impl.hxx:1206-1216), so the values are bit-identical to
 // the reference's; only the number of times a shared 1-D result is evaluated
 // changes.
+//
+// The body (stream_body.cuh) is compiled for two CTA sizes: namespace big
+// (256 threads, 512 units per item) and namespace small (128 threads, 256
+// units) for boxes with at most 256 units per x chunk.  In a level, CTAs
+// take items from a per-launch counter, and each launch after a plan's
+// first is a programmatic dependent of the previous one.
 #pragma once
 #include "cx_internal.h"
 #include "cx_stencils.cuh"
