@@ -9,13 +9,14 @@ namespace cxb {
 
 // Streaming kernel: threads per CTA (kStrThreadsSmall for the items of
 // boxes with at most kStrSmallUnits column units per x chunk), column units
-// per thread; at most kStrPairRows pairs of fine y rows and kStrMaxWidth fine
-// x per item.
+// per thread, fine y per unit (kStrFineYPerUnit / 2 coarse y centres); at
+// most kStrUnitRows rows of units and kStrMaxWidth fine x per item.
 constexpr int kStrThreads = 256;
 constexpr int kStrThreadsSmall = 128;
-constexpr int kStrSmallUnits = 256;
-constexpr int kStrUnitsPerThread = 2;
-constexpr int kStrPairRows = 64;
+constexpr int kStrUnitsPerThread = 1;
+constexpr int kStrFineYPerUnit = 4;
+constexpr int kStrSmallUnits = kStrThreadsSmall * kStrUnitsPerThread;
+constexpr int kStrUnitRows = 32;
 constexpr int kStrMaxWidth = 130;
 
 // One box of a transfer as the kernels see it.  Coordinates are AMReX index
@@ -38,7 +39,7 @@ struct BoxDesc {
   int ncomp;
   int zchunk;         // streaming kernel: fine z per item (even)
   int xcw;            // streaming kernel: fine x per x chunk
-  int npr;            // streaming kernel: pairs of fine y rows
+  int npr;            // streaming kernel: rows of units (kStrFineYPerUnit fine y)
   int upi;            // streaming kernel: units (columns) per item
   int scta;           // streaming kernel: 1 = the 128-thread variant
   double *cbar;       // adjoint: coarse output (P^T fine)

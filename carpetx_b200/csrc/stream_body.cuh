@@ -8,8 +8,9 @@
 constexpr int NTS = CXS_NTS;    // threads per CTA (256, or 128 for small items)
 constexpr int UPT = kStrUnitsPerThread; // column units per thread
 constexpr int NU = NTS * UPT;    // column units per item
-constexpr int FYT = 2;           // fine y per unit (one coarse y centre)
-constexpr int PRMAX = kStrPairRows; // pair rows per item at most
+constexpr int FYT = kStrFineYPerUnit; // fine y per unit
+constexpr int CYU = FYT / 2;     // coarse y centres per unit
+constexpr int PRMAX = kStrUnitRows; // rows of units per item at most
 constexpr int WFMAX = kStrMaxWidth; // fine x per x chunk at most
 constexpr int DPF = 3;           // coarse planes prefetched ahead
 constexpr int NRING = DPF + 1;   // shared-memory plane ring
@@ -19,8 +20,9 @@ constexpr int XB = 4;            // fine x per x-pass task
 // Geometry of an item whose x chunk is W fine points wide (worst case over
 // the stencil kinds): rows of the coarse window / x-pass result, their
 // pitches, x-pass tasks.
+// coarse y centres an item of W-wide unit rows spans at most
 __host__ __device__ constexpr int span_rows(int W) {
-  return PRMAX < (NU - 1) / W + 2 ? PRMAX : (NU - 1) / W + 2;
+  return CYU * (PRMAX < (NU - 1) / W + 2 ? PRMAX : (NU - 1) / W + 2);
 }
 __host__ __device__ constexpr int nseg_of(int W) { return (W + XB - 1) / XB; }
 __host__ __device__ constexpr int p0_of(int W, int wx) { return (nseg_of(W) * XB / 2 + wx) | 1; }
@@ -74,17 +76,20 @@ __device__ __forceinline__ void xtask(const double *__restrict__ src, double *__
   }
 }
 
-// y pass of one unit: its 2 fine y share the coarse y window starting at
-// src (rows pxw apart).
+// y pass of one unit: its FYT fine y (CYU coarse y centres, 2 fine y each)
+// from the coarse y window starting at src (rows pxw apart).
 template <class K>
-__device__ __forceinline__ void ypass(const double *__restrict__ src, int pxw, double y[2]) {
-  constexpr int W = 1 + K::RHI - K::RLO;
+__device__ __forceinline__ void ypass(const double *__restrict__ src, int pxw, double y[FYT]) {
+  constexpr int W = CYU + K::RHI - K::RLO;
   double v[W];
 #pragma unroll
   for (int i = 0; i < W; ++i)
     v[i] = src[i * pxw];
-  y[0] = K::template ap<0>(v - K::RLO);
-  y[1] = K::template ap<1>(v - K::RLO);
+#pragma unroll
+  for (int c = 0; c < CYU; ++c) {
+    y[2 * c] = K::template ap<0>(v + c - K::RLO);
+    y[2 * c + 1] = K::template ap<1>(v + c - K::RLO);
+  }
 }
 
 // Per-item, per-thread geometry shared by all planes.
@@ -223,7 +228,7 @@ __device__ __forceinline__ void stream_item(Shared &sh, const Item &it) {
 
 // Geometry of work item (x chunk, unit block, z chunk, comp) of box b, for
 // the z kind's streaming window [zwlo, zwhi].
-// The item's units are the unit block's consecutive (pair row, fine x)
+// The item's units are the unit block's consecutive (unit row, fine x)
 // columns of the x chunk, flattened x fastest; thread t owns unit t.
 // Returns false if the block holds no unit (box mode, narrow last chunk).
 __device__ __forceinline__ bool make_item(const BoxDesc &b, int xchunk, int ublock, int zchunk,
@@ -238,13 +243,13 @@ __device__ __forceinline__ bool make_item(const BoxDesc &b, int xchunk, int ublo
   const int uend = min(u0 + b.upi, nunits);
   const int pr_lo = u0 / W, pr_hi = (uend - 1) / W;
   const int rlx = sep_rlo(kx), rly = sep_rlo(ky);
-  const int NR = pr_hi - pr_lo + 1 + sep_rhi(ky) - rly;
+  const int NR = (pr_hi - pr_lo + 1) * CYU + sep_rhi(ky) - rly;
   const int nseg = nseg_of(W);
   const int Wx = (W - 1) / 2 + 1 + sep_rhi(kx) - rlx;
   const int P0 = p0_of(W, sep_rhi(kx) - rlx);
   it.pxw = pxw_of(W);
   const int cxb = xb / 2 + rlx;                   // xb even
-  const int cyb = b.tbase[1] / 2 + pr_lo + rly;   // tbase even
+  const int cyb = b.tbase[1] / 2 + pr_lo * CYU + rly; // tbase even
   it.cbase = b.crse + comp * b.cnp;
   it.cplane = (int64_t)b.cnx * b.cny;
   it.clo_z = b.clo[2];
@@ -267,8 +272,8 @@ __device__ __forceinline__ bool make_item(const BoxDesc &b, int xchunk, int ublo
     it.col[q] = b.fine;
     if (u < uend) {
       const int pr = u / W, fxl = u - pr * W;
-      const int fx = xb + fxl, fy0 = b.tbase[1] + 2 * pr;
-      it.ysrc[q] = (pr - pr_lo) * it.pxw + fxl;
+      const int fx = xb + fxl, fy0 = b.tbase[1] + FYT * pr;
+      it.ysrc[q] = (pr - pr_lo) * CYU * it.pxw + fxl;
       if (fx >= b.rlo[0]) {
 #pragma unroll
         for (int j = 0; j < FYT; ++j)

@@ -6,16 +6,16 @@
 // window.
 //
 // A work item is one component of a block of up to NU fine "units" of a box
-// over a chunk of fine z; a unit is a column (fine x, pair of fine y sharing
-// a coarse y centre), units are numbered x fastest over the box's x chunk
-// (any width up to WFMAX), so every lane works on a real fine point whatever
-// the box shape.  The CTA streams the coarse z planes of the block's window
+// over a chunk of fine z; a unit is a fine x with FYT fine y (FYT / 2
+// coarse y centres, whose y windows overlap), units are numbered x fastest
+// over the box's x chunk (any width up to WFMAX), so every lane works on a
+// real fine point whatever the box shape.  The CTA streams the coarse z planes of the block's window
 // through a ring of shared-memory planes:
 //   load    plane c + DPF of the coarse window (asynchronous 8-byte copies,
 //           zero-filled outside the coarse points the operator reads);
 //   x pass  X[cy][fx] = interp_x(coarse row), XB fine x per task from a
 //           register window, into shared memory;
-//   y pass  each thread computes Y for the 2 fine y of each of its UPT
+//   y pass  each thread computes Y for the FYT fine y of each of its UPT
 //           units from a register window of X (consecutive lanes =
 //           consecutive fine x);
 //   z pass  each thread keeps the Y values of the last L coarse planes in a
@@ -33,8 +33,8 @@
 // changes.
 //
 // The body (stream_body.cuh) is compiled for two CTA sizes: namespace big
-// (256 threads, 512 units per item) and namespace small (128 threads, 256
-// units) for boxes with at most 256 units per x chunk.  In a level, CTAs
+// (256 threads, 256 units per item) and namespace small (128 threads, 128
+// units) for boxes with at most 128 units per x chunk.  In a level, CTAs
 // take items from a per-launch counter, and each launch after a plan's
 // first is a programmatic dependent of the previous one.
 #pragma once

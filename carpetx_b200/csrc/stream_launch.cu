@@ -91,7 +91,7 @@ void stream_tiling(BoxDesc &b, int min_items) {
   for (int d = 0; d < 3; ++d)
     b.tbase[d] = b.rlo[d] & ~1;
   // x chunks: the whole width up to kStrMaxWidth, else near-equal even chunks
-  constexpr int WFMAX = kStrMaxWidth, PRMAX = kStrPairRows;
+  constexpr int WFMAX = kStrMaxWidth, PRMAX = kStrUnitRows;
   const int Wt = b.rhi[0] - b.tbase[0] + 1;
   if (Wt <= WFMAX) {
     b.xcw = Wt;
@@ -103,7 +103,7 @@ void stream_tiling(BoxDesc &b, int min_items) {
     b.xcw = w;
     b.ntile[0] = (Wt + w - 1) / w;
   }
-  b.npr = (b.rhi[1] - b.tbase[1]) / 2 + 1;
+  b.npr = (b.rhi[1] - b.tbase[1]) / kStrFineYPerUnit + 1;
   // boxes with at most kStrSmallUnits column units per x chunk run on the
   // 128-thread variant (one item of 256 unit slots instead of 512)
   b.scta = b.npr * b.xcw <= kStrSmallUnits ? 1 : 0;
