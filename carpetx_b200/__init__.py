@@ -54,6 +54,51 @@ class CxBox(ctypes.Structure):
                 ("reg_lo", _I3), ("reg_hi", _I3)]
 
 
+# symmetries and boundary conditions (CarpetX driver.hxx:41-57)
+SYM_NONE, SYM_INTERPATCH, SYM_PERIODIC, SYM_REFLECTION = range(4)
+BC_NONE, BC_SYMMETRY_BOUNDARY, BC_DIRICHLET, BC_LINEAR_EXTRAPOLATION, BC_NEUMANN, BC_ROBIN = range(6)
+BC_MAX_COMPS = 16
+_D3 = ctypes.c_double * 3
+
+
+class CxBc(ctypes.Structure):
+    """cx_bc_t"""
+    _fields_ = [("symmetry", _I3 * 2), ("boundary", _I3 * 2), ("domain_lo", _I3),
+                ("domain_hi", _I3), ("prob_lo", _D3), ("prob_hi", _D3), ("dx", _D3),
+                ("indextype", _I3), ("nghost", _I3), ("ncomp", _I),
+                ("dirichlet", ctypes.c_double * BC_MAX_COMPS),
+                ("robin", ctypes.c_double * BC_MAX_COMPS), ("parity", _I3 * BC_MAX_COMPS)]
+
+
+class CxBcFab(ctypes.Structure):
+    """cx_bc_fab_t"""
+    _fields_ = [("data", _VP), ("lo", _I3), ("hi", _I3)]
+
+
+def bc_struct(spec):
+    """cx_bc_t from a dict: symmetry, boundary ([face][dir] nested lists),
+    domain_lo, domain_hi, prob_lo, prob_hi, dx, indextype, nghost (optional,
+    default 0) and per component dirichlet, robin, parity (ncomp x 3)."""
+    b = CxBc()
+    n = len(spec["dirichlet"])
+    if not 1 <= n <= BC_MAX_COMPS or len(spec["robin"]) != n or len(spec["parity"]) != n:
+        raise ValueError(f"1..{BC_MAX_COMPS} components with dirichlet, robin and parity each")
+    for f in range(2):
+        b.symmetry[f] = _i3(spec["symmetry"][f])
+        b.boundary[f] = _i3(spec["boundary"][f])
+    b.domain_lo, b.domain_hi = _i3(spec["domain_lo"]), _i3(spec["domain_hi"])
+    b.prob_lo, b.prob_hi = _D3(*spec["prob_lo"]), _D3(*spec["prob_hi"])
+    b.dx = _D3(*spec["dx"])
+    b.indextype = _i3(spec["indextype"])
+    b.nghost = _i3(spec.get("nghost", (0, 0, 0)))
+    b.ncomp = n
+    for c in range(n):
+        b.dirichlet[c] = float(spec["dirichlet"][c])
+        b.robin[c] = float(spec["robin"][c])
+        b.parity[c] = _i3(spec["parity"][c])
+    return b
+
+
 def lib():
     """The loaded C library (raises if it was not built)."""
     global _lib
@@ -84,6 +129,13 @@ def lib():
         L.cx_restrict_adjoint_box.argtypes = [_I, _VP, _I3, _I3, _VP, _I3, _I3, _I3, _I3, _I, _VP]
         L.cx_prolong_adjoint_box.argtypes = [ctypes.c_int32, _VP, _I3, _I3, _VP, _I3, _I3, _I3,
                                              _I3, _I, _I, _VP, _VP]
+        L.cx_boundary_box.argtypes = [ctypes.POINTER(CxBc), _VP, _I3, _I3, _VP]
+        L.cx_boundary_plan_create.argtypes = [ctypes.POINTER(CxBc), ctypes.POINTER(CxBcFab), _I,
+                                              ctypes.POINTER(_VP)]
+        L.cx_boundary_plan_execute.argtypes = [_VP, _VP]
+        L.cx_boundary_plan_stats.argtypes = [_VP, ctypes.POINTER(ctypes.c_int64),
+                                             ctypes.POINTER(ctypes.c_int64)]
+        L.cx_boundary_plan_destroy.argtypes = [_VP]
         _lib = L
     return _lib
 
@@ -191,6 +243,51 @@ def restrict_adjoint_box(indextype, crse_bar, crse_lo, crse_hi, fine_bar, fine_l
         int(indextype), _ptr(crse_bar, ncomp, crse_lo, crse_hi, "crse_bar"), _i3(crse_lo),
         _i3(crse_hi), _ptr(fine_bar, ncomp, fine_lo, fine_hi, "fine_bar"), _i3(fine_lo),
         _i3(fine_hi), _i3(reg_lo), _i3(reg_hi), int(ncomp), _stream(stream)))
+
+
+def boundary_box(spec, data, lo, hi, stream=None):
+    """cx_boundary_box: the outer boundary conditions of one FAB, in place
+    (asynchronous).  spec as for bc_struct."""
+    b = bc_struct(spec)
+    _check(lib().cx_boundary_box(ctypes.byref(b), _ptr(data, b.ncomp, lo, hi, "data"), _i3(lo),
+                                 _i3(hi), _stream(stream)))
+
+
+class BoundaryPlan:
+    """cx_boundary_plan_*: the outer boundary conditions of every FAB of a
+    level (GroupData::apply_boundary_conditions) as one launch.  fabs:
+    iterable of (tensor, lo, hi); the plan keeps the tensors alive."""
+
+    def __init__(self, spec, fabs):
+        b = bc_struct(spec)
+        fabs = list(fabs)
+        arr = (CxBcFab * max(1, len(fabs)))()
+        self._keep = []
+        for i, (t, lo, hi) in enumerate(fabs):
+            arr[i] = CxBcFab(_ptr(t, b.ncomp, lo, hi, "fab").value, _i3(lo), _i3(hi))
+            self._keep.append(t)
+        h = ctypes.c_void_p()
+        _check(lib().cx_boundary_plan_create(ctypes.byref(b), arr, len(fabs), ctypes.byref(h)))
+        self.handle = h
+
+    def execute(self, stream=None):
+        _check(lib().cx_boundary_plan_execute(self.handle, _stream(stream)))
+
+    def stats(self):
+        a, c = ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().cx_boundary_plan_stats(self.handle, ctypes.byref(a), ctypes.byref(c)))
+        return {"points": a.value, "bytes": c.value}
+
+    def close(self):
+        if self.handle:
+            lib().cx_boundary_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class LevelPlan:

@@ -50,3 +50,63 @@ def mixed_level_boxes(seed, nboxes=512, cmin=8, cmax=64, ghosts=3):
         fhi = tuple(int(2 * n[d] - 1 + (1 - cc[d])) for d in range(3))
         out.append((it, clo, chi, flo, fhi))
     return out
+
+
+# face conditions (symmetry, boundary) that CarpetX accepts on a face
+# (boundaries_impl.hxx:71-108), periodic excluded (it pairs both faces)
+BC_FACE_CHOICES = [(0, 0), (1, 0), (3, 0), (3, 1), (0, 2), (0, 3), (0, 4), (0, 5), (1, 2),
+                   (1, 3), (1, 4), (1, 5)]
+
+
+def boundary_spec(rng, ncomp, indextype, domain_n, nghost=3, faces=None, periodic=(False,) * 3):
+    """A group's outer conditions on a level whose cell-centred domain is
+    0..domain_n[d]-1: per face (symmetry, boundary) drawn from
+    BC_FACE_CHOICES unless `faces` ([face][dir] pairs) is given, periodic
+    directions periodic on both faces; physical box [0.123, 0.123 + n dx]
+    with dx = 0.0371 (no grid point at the origin); per component Dirichlet
+    values, Robin values at infinity and reflection parities drawn at
+    random."""
+    sym = [[0] * 3 for _ in range(2)]
+    bc = [[0] * 3 for _ in range(2)]
+    for f in range(2):
+        for d in range(3):
+            s, b = faces[f][d] if faces is not None else \
+                BC_FACE_CHOICES[rng.integers(len(BC_FACE_CHOICES))]
+            if periodic[d]:
+                s, b = 2, 0
+            sym[f][d], bc[f][d] = int(s), int(b)
+    dx = 0.0371
+    return {
+        "symmetry": sym, "boundary": bc,
+        "domain_lo": (0, 0, 0), "domain_hi": tuple(int(n) - 1 for n in domain_n),
+        "prob_lo": (0.123,) * 3, "prob_hi": tuple(0.123 + int(n) * dx for n in domain_n),
+        "dx": (dx,) * 3, "indextype": tuple(int(v) for v in indextype),
+        "nghost": (nghost,) * 3,
+        "dirichlet": rng.uniform(-2, 2, ncomp).tolist(),
+        "robin": rng.uniform(-1, 1, ncomp).tolist(),
+        "parity": rng.choice([-1, 1], (ncomp, 3)).tolist(),
+    }
+
+
+def tiled_level_fabs(domain_n, box_n, indextype, nghost):
+    """FABs (lo, hi) of a level whose domain 0..domain_n-1 is tiled by boxes
+    of box_n cells per direction, each grown by nghost (vertex-centred
+    directions hold the closing vertex too)."""
+    out = []
+    nb = [int(domain_n[d]) // int(box_n[d]) for d in range(3)]
+    for k in range(nb[2]):
+        for j in range(nb[1]):
+            for i in range(nb[0]):
+                t = (i, j, k)
+                lo = tuple(t[d] * box_n[d] - nghost for d in range(3))
+                hi = tuple((t[d] + 1) * box_n[d] - 1 + (1 - indextype[d]) + nghost
+                           for d in range(3))
+                out.append((lo, hi))
+    return out
+
+
+# The level of the boundary-condition benchmark: a 256^3-cell domain in 512
+# FABs of 32^3 cells with 3 ghosts, 16 cell-centred components, and every
+# kind of condition: reflection (x lower), Dirichlet (x upper), linear
+# extrapolation (y lower, z upper), Robin (y upper), Neumann (z lower).
+BC_LEVEL_FACES = [[(3, 0), (0, 3), (0, 4)], [(0, 2), (0, 5), (0, 3)]]

@@ -228,6 +228,84 @@ int cx_restrict_adjoint_box(int indextype, const double *crse_bar,
                             const int reg_hi[3], int ncomp,
                             cx_stream_t stream);
 
+/* ---- Outer boundary conditions --------------------------------------------
+ * The step after a prolongation in CarpetX's sync: points of a FAB outside
+ * the domain interior are set from its symmetries and boundary conditions,
+ * as BoundaryCondition(groupdata, dest).apply() does (CarpetX/src/
+ * boundaries.cxx:32-118, boundaries_impl.hxx:28-444).
+ *
+ * The interior is the domain's cells, or its vertices in vertex-centred
+ * directions: [domain_lo, domain_hi + 1 + !indextype).  A face's condition
+ * is chosen as in apply_on_face (boundaries_impl.hxx:71-108): periodic
+ * faces, and faces with no or an inter-patch symmetry and no boundary
+ * condition, set nothing; reflection symmetry takes precedence over the
+ * group's condition.  On edges and corners the conditions of all boundary
+ * directions combine: Dirichlet sets the value; otherwise the value is read
+ * at the source point (the interior edge point in Neumann, Robin and
+ * linear-extrapolation directions, the mirror point in reflection
+ * directions), then the Robin fall-off, the linear extrapolation and the
+ * reflection parity are applied, in that order, with the reference's
+ * rounding.  Every point written reads only points that are not written, so
+ * one launch covers all regions of all FABs.
+ *
+ * Symmetries (PatchData::symmetries) and boundary conditions
+ * (GroupData::boundaries) with CarpetX's numbering (driver.hxx:41-57). */
+enum { CX_SYM_NONE = 0, CX_SYM_INTERPATCH = 1, CX_SYM_PERIODIC = 2, CX_SYM_REFLECTION = 3 };
+enum {
+  CX_BC_NONE = 0,
+  CX_BC_SYMMETRY_BOUNDARY = 1,
+  CX_BC_DIRICHLET = 2,
+  CX_BC_LINEAR_EXTRAPOLATION = 3,
+  CX_BC_NEUMANN = 4,
+  CX_BC_ROBIN = 5
+};
+#define CX_BC_MAX_COMPS 16 /* maxncomps, boundaries_impl.hxx:30 */
+
+/* A group's conditions on one level. */
+typedef struct {
+  int symmetry[2][3];               /* [face: 0 lower, 1 upper][direction], CX_SYM_* */
+  int boundary[2][3];               /* CX_BC_*, same indexing */
+  int domain_lo[3], domain_hi[3];   /* Geometry::Domain(): cell-centred, inclusive */
+  double prob_lo[3], prob_hi[3];    /* Geometry::ProbLo / ProbHi */
+  double dx[3];                     /* Geometry::CellSize */
+  int indextype[3];                 /* 1: cell centred in direction d */
+  int nghost[3];                    /* MultiFab::nGrow of the level's FABs */
+  int ncomp;                        /* 1..CX_BC_MAX_COMPS */
+  double dirichlet[CX_BC_MAX_COMPS]; /* GroupData::dirichlet_values */
+  double robin[CX_BC_MAX_COMPS];    /* GroupData::robin_values (value at infinity) */
+  int parity[CX_BC_MAX_COMPS][3];   /* GroupData::parities: +1 or -1 */
+} cx_bc_t;
+
+/* One FAB of the level: device data (ncomp components) on [lo, hi]. */
+typedef struct {
+  double *data;
+  int lo[3], hi[3];
+} cx_bc_fab_t;
+
+/* BoundaryCondition(groupdata, dest).apply() on one FAB: one launch, no
+ * allocation.  CX_EINVAL for a face whose symmetry and condition do not
+ * combine (the reference's "internal error"), ncomp out of range, a
+ * parity other than +-1, or a source point outside the FAB or outside the
+ * interior (the reference asserts the first and does not check the second,
+ * which only a domain narrower than the ghost zones can violate). */
+int cx_boundary_box(const cx_bc_t *bc, double *data, const int lo[3], const int hi[3],
+                    cx_stream_t stream);
+
+/* GroupData::apply_boundary_conditions (driver.cxx:967-995) for every FAB of
+ * a level in one launch.  Nothing is done when every direction is periodic;
+ * FABs inside the domain grown by nghost in its periodic directions are
+ * skipped.  The plan holds the device list of regions; FABs must not
+ * overlap.  Create once per regrid, execute every sync (no allocation,
+ * graph-capturable). */
+typedef struct cx_boundary_plan *cx_boundary_plan_t;
+int cx_boundary_plan_create(const cx_bc_t *bc, const cx_bc_fab_t *fabs, int nfabs,
+                            cx_boundary_plan_t *out);
+int cx_boundary_plan_execute(cx_boundary_plan_t plan, cx_stream_t stream);
+/* Points set per execution (over all components: npoints x ncomp values)
+ * and algorithmic bytes: 8 written per value, plus 8 read unless Dirichlet. */
+int cx_boundary_plan_stats(cx_boundary_plan_t plan, int64_t *npoints, int64_t *bytes);
+int cx_boundary_plan_destroy(cx_boundary_plan_t plan);
+
 #ifdef __cplusplus
 }
 #endif

@@ -949,3 +949,152 @@ int cxo_restrict_adjoint(int indextype, const double *crse_bar,
         }
   return 0;
 }
+
+/* ---- Outer boundary conditions ------------------------------------------
+ * Restates CarpetX's BoundaryCondition (boundaries.cxx:32-118,
+ * boundaries_impl.hxx:28-444).  The reference visits the 26 regions of the
+ * destination box outside the domain interior [imin, imax) (below, inside or
+ * above it per direction) one template instantiation each; here each point
+ * finds its region from its coordinates, which is the same partition. */
+enum { BM_NONE, BM_DIRICHLET, BM_LINEXT, BM_NEUMANN, BM_ROBIN, BM_REFLECT, BM_BAD };
+
+/* Condition of direction d on face f (0 lower, 1 upper), as chosen in
+ * apply_on_face (boundaries_impl.hxx:71-108): periodic faces, and faces with
+ * no or an inter-patch symmetry and no boundary condition, set nothing; a
+ * reflection symmetry takes precedence over the group's boundary condition;
+ * any other combination is an internal error there. */
+static int bc_mode(const int sym[6], const int bc[6], int f, int d) {
+  const int s = sym[3 * f + d], b = bc[3 * f + d];
+  if (((s == 0 || s == 1) && b == 0) || s == 2)
+    return BM_NONE;
+  if (s == 3)
+    return BM_REFLECT;
+  switch (b) {
+  case 2: return BM_DIRICHLET;
+  case 3: return BM_LINEXT;
+  case 4: return BM_NEUMANN;
+  case 5: return BM_ROBIN;
+  default: return BM_BAD;
+  }
+}
+
+int cxo_boundary_box(const int symmetry[6], const int boundary[6],
+                     const int domain_lo[3], const int domain_hi[3],
+                     const double prob_lo[3], const double prob_hi[3],
+                     const double dx[3], const int indextype[3], int ncomp,
+                     const double *dirichlet, const double *robin,
+                     const int *parity, double *data, const int lo[3],
+                     const int hi[3]) {
+  (void)prob_hi;
+  if (ncomp < 1 || ncomp > 16 || !box_ok(lo, hi))
+    return -1;
+  int imin[3], imax[3], nx[3];
+  double xmin[3];
+  for (int d = 0; d < 3; ++d) {
+    /* interior: the domain's cells, or its vertices (one more), as in the
+     * constructor (boundaries.cxx:40-48); xmin as written there */
+    imin[d] = domain_lo[d];
+    imax[d] = domain_hi[d] + 1 + !indextype[d];
+    xmin[d] = prob_lo[d] + 0.5 * indextype[d] - 1;
+    nx[d] = hi[d] - lo[d] + 1;
+  }
+  const long np = (long)nx[0] * nx[1] * nx[2];
+#define AT(c, q) data[(c) * np + ((q)[0] - lo[0]) + nx[0] * (((q)[1] - lo[1]) + nx[1] * (long)((q)[2] - lo[2]))]
+  /* pass 0 checks every region; pass 1 writes.  Sources lie inside the
+   * interior in every direction that has a condition, so no point read is
+   * one that is written. */
+  for (int pass = 0; pass < 2; ++pass)
+    for (int k = lo[2]; k <= hi[2]; ++k)
+      for (int j = lo[1]; j <= hi[1]; ++j)
+        for (int i = lo[0]; i <= hi[0]; ++i) {
+          const int p[3] = {i, j, k};
+          int r[3], m[3], src[3], sp[3], delta[3] = {0, 0, 0};
+          int any = 0, flags = 0;
+          for (int d = 0; d < 3; ++d) {
+            r[d] = p[d] < imin[d] ? -1 : p[d] >= imax[d] ? 1 : 0;
+            m[d] = r[d] ? bc_mode(symmetry, boundary, r[d] > 0, d) : BM_NONE;
+            if (m[d] == BM_BAD)
+              return -1;
+            any |= m[d] != BM_NONE;
+            flags |= 1 << m[d];
+          }
+          if (!any)
+            continue;
+          for (int d = 0; d < 3; ++d) {
+            const int edge = r[d] < 0 ? imin[d] : imax[d] - 1;
+            src[d] = p[d];
+            switch (m[d]) {
+            case BM_LINEXT: src[d] = edge; delta[d] = -r[d]; break;
+            case BM_NEUMANN:
+            case BM_ROBIN: src[d] = edge; break;
+            case BM_REFLECT:
+              src[d] = (r[d] < 0 ? 2 * imin[d] - indextype[d]
+                                 : 2 * (imax[d] - 1) + indextype[d]) - p[d];
+              break;
+            default: break;
+            }
+            sp[d] = src[d] + delta[d];
+          }
+          if (pass == 0) {
+            for (int d = 0; d < 3; ++d) {
+              if (m[d] == BM_NONE || m[d] == BM_DIRICHLET)
+                continue;
+              if (src[d] < imin[d] || src[d] >= imax[d] || src[d] < lo[d] || src[d] > hi[d] ||
+                  sp[d] < imin[d] || sp[d] >= imax[d] || sp[d] < lo[d] || sp[d] > hi[d])
+                return -1;
+            }
+            if (flags & (1 << BM_REFLECT))
+              for (int c = 0; c < ncomp; ++c)
+                for (int d = 0; d < 3; ++d)
+                  if (m[d] == BM_REFLECT && parity[3 * c + d] != 1 && parity[3 * c + d] != -1)
+                    return -1;
+            continue;
+          }
+          for (int c = 0; c < ncomp; ++c) {
+            double val;
+            if (flags & (1 << BM_DIRICHLET)) {
+              val = dirichlet[c];
+            } else {
+              val = AT(c, src);
+              if (flags & (1 << BM_ROBIN))
+                /* f(x') = finf + |x| / |x'| (f(x) - finf), once per Robin
+                 * direction (boundaries_impl.hxx:391-408) */
+                for (int d = 0; d < 3; ++d) {
+                  if (m[d] != BM_ROBIN)
+                    continue;
+                  double sb = 0, si = 0;
+                  for (int e = 0; e < 3; ++e) {
+                    const double xb = xmin[e] + p[e] * dx[e];
+                    const double xi = xmin[e] + src[e] * dx[e];
+                    sb = sb + xb * xb;
+                    si = si + xi * xi;
+                  }
+                  const double q = sqrt(si) / sqrt(sb);
+                  val = robin[c] + q * (val - robin[c]);
+                }
+              if (flags & (1 << BM_LINEXT)) {
+                /* slope from the two points src, src + delta; the distance
+                 * ratio is an integer quotient of squared lengths, taken
+                 * before the square root (boundaries_impl.hxx:409-414) */
+                const double grad = val - AT(c, sp);
+                int n2 = 0, d2 = 0;
+                for (int d = 0; d < 3; ++d) {
+                  n2 += (p[d] - src[d]) * (p[d] - src[d]);
+                  d2 += delta[d] * delta[d];
+                }
+                val = val + sqrt((double)(n2 / d2)) * grad;
+              }
+              if (flags & (1 << BM_REFLECT)) {
+                double par = 1;
+                for (int d = 0; d < 3; ++d)
+                  if (m[d] == BM_REFLECT)
+                    par = par * parity[3 * c + d];
+                val = val * par;
+              }
+            }
+            AT(c, p) = val;
+          }
+        }
+#undef AT
+  return 0;
+}

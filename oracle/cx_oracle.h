@@ -86,6 +86,23 @@ int cxo_restrict_adjoint(int indextype, const double *crse_bar,
                          const int fine_hi[3], const int reg_lo[3],
                          const int reg_hi[3], int ncomp);
 
+/* Outer boundary conditions of one FArrayBox [lo, hi] (ncomp components,
+ * at most 16), restating BoundaryCondition(groupdata, dest).apply()
+ * (CarpetX/src/boundaries.cxx, boundaries_impl.hxx).  symmetry[3f+d] and
+ * boundary[3f+d] are CarpetX's symmetry_t / boundary_t values (driver.hxx:
+ * 41-57) of face f (0 lower, 1 upper) in direction d; domain_lo/hi is the
+ * level's cell-centred domain box; indextype[d] = 1 for cell centred;
+ * parity[3c+d] the reflection parity of component c.  Writes the points
+ * outside the domain interior; returns -1 (nothing written) for an invalid
+ * condition or a source point outside the box or the interior. */
+int cxo_boundary_box(const int symmetry[6], const int boundary[6],
+                     const int domain_lo[3], const int domain_hi[3],
+                     const double prob_lo[3], const double prob_hi[3],
+                     const double dx[3], const int indextype[3], int ncomp,
+                     const double *dirichlet, const double *robin,
+                     const int *parity, double *data, const int lo[3],
+                     const int hi[3]);
+
 /* The 1-D coefficient row used by the oracle for (cent, intp, order), row
  * `row` for ENO (0..order), exact dyadic values; returns the number of
  * coefficients written (0 if the stencil is not defined). */

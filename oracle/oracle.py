@@ -10,6 +10,14 @@ Two oracles:
 * ``RefOracle`` -- ``_ref/libref_prolong.so``, the reference operators
   (CarpetX/src/prolongate_3d_rf2*.cxx) compiled unmodified; present when the
   reference tree was available at build time.
+* ``RefBoundary`` -- ``_ref/libref_bc.so``, the reference outer boundary
+  conditions (CarpetX/src/boundaries*.cxx) compiled unmodified, same proviso.
+
+Boundary conditions take a ``spec`` dict: ``symmetry`` and ``boundary``
+(2 x 3 nested lists of CarpetX's symmetry_t / boundary_t values, [face][dir]),
+``domain_lo``/``domain_hi`` (cell-centred domain box), ``prob_lo``,
+``prob_hi``, ``dx``, ``indextype`` (1 = cell centred), and per component
+``dirichlet``, ``robin`` and ``parity`` (ncomp x 3 of +-1).
 
 Arrays are numpy float64, Fortran-ordered FAB layout flattened as
 ``(ncomp, nz, ny, nx)`` C-contiguous (x fastest, component stride = box points).
@@ -52,6 +60,28 @@ def box_shape(lo, hi):
     return tuple(int(hi[d]) - int(lo[d]) + 1 for d in (2, 1, 0))
 
 
+_BC_ARGTYPES = [ctypes.c_int * 6, ctypes.c_int * 6, _I3, _I3, ctypes.c_double * 3,
+                ctypes.c_double * 3, ctypes.c_double * 3, _I3, ctypes.c_int, _DP, _DP,
+                ctypes.POINTER(ctypes.c_int), _DP, _I3, _I3]
+
+
+def _bc_call(fn, spec, data, lo, hi):
+    """Calls a boundary-condition entry with the signature of
+    cxo_boundary_box / ref_boundary_box on data (ncomp, nz, ny, nx)."""
+    D3 = ctypes.c_double * 3
+    ncomp = len(spec["dirichlet"])
+    assert data.shape == (ncomp,) + box_shape(lo, hi)
+    sym = (ctypes.c_int * 6)(*[int(v) for f in spec["symmetry"] for v in f])
+    bc = (ctypes.c_int * 6)(*[int(v) for f in spec["boundary"] for v in f])
+    dirv = np.ascontiguousarray(spec["dirichlet"], dtype=np.float64)
+    rob = np.ascontiguousarray(spec["robin"], dtype=np.float64)
+    par = np.ascontiguousarray(spec["parity"], dtype=np.int32).reshape(-1)
+    return fn(sym, bc, _i3(spec["domain_lo"]), _i3(spec["domain_hi"]), D3(*spec["prob_lo"]),
+              D3(*spec["prob_hi"]), D3(*spec["dx"]), _i3(spec["indextype"]), ncomp, _dp(dirv),
+              _dp(rob), par.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(data), _i3(lo),
+              _i3(hi))
+
+
 class CxOp(ctypes.Structure):
     _fields_ = [("cent", ctypes.c_int * 3), ("intp", ctypes.c_int * 3),
                 ("order", ctypes.c_int * 3), ("fb", ctypes.c_int)]
@@ -77,6 +107,7 @@ class CxOracle:
         L.cxo_coarse_box.argtypes = [ctypes.POINTER(CxOp), _I3, _I3, _I3, _I3]
         L.cxo_required_ghosts.argtypes = [ctypes.POINTER(CxOp), _I3]
         L.cxo_coeffs.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _DP]
+        L.cxo_boundary_box.argtypes = _BC_ARGTYPES
 
     def op(self, typ, order, indextype):
         o = CxOp()
@@ -141,6 +172,33 @@ class CxOracle:
                                            int(ncomp))
         if rc != 0:
             raise ValueError("cxo_restrict_adjoint rejected its arguments")
+
+
+    def boundary(self, spec, data, lo, hi):
+        """Outer boundary conditions of one FAB, in place (cxo_boundary_box)."""
+        if _bc_call(self.lib.cxo_boundary_box, spec, data, lo, hi) != 0:
+            raise ValueError("cxo_boundary_box rejected its arguments")
+
+
+class RefBoundary:
+    """The reference boundary conditions compiled unmodified (oracle/_ref)."""
+
+    PATH = os.path.join(HERE, "_ref", "libref_bc.so")
+
+    def __init__(self):
+        if not os.path.exists(self.PATH):
+            raise RuntimeError(f"reference oracle not built: {self.PATH}")
+        self.lib = ctypes.CDLL(self.PATH)
+        self.lib.ref_boundary_box.argtypes = _BC_ARGTYPES
+
+    @classmethod
+    def available(cls):
+        return os.path.exists(cls.PATH)
+
+    def boundary(self, spec, data, lo, hi):
+        """BoundaryCondition(groupdata, dest).apply() on one FAB, in place."""
+        if _bc_call(self.lib.ref_boundary_box, spec, data, lo, hi) != 0:
+            raise ValueError("ref_boundary_box rejected its arguments")
 
 
 class RefOracle:

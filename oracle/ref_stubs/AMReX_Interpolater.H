@@ -1,5 +1,6 @@
-/* Minimal stand-in for the AMReX types the reference transfer operators use
- * (Box, IntVect, FArrayBox, ParallelFor and the Interpolater base class).
+/* Minimal stand-in for the AMReX types the reference transfer operators and
+ * boundary conditions use (Box with its index type, IntVect, FArrayBox,
+ * Geometry, ParallelFor and the Interpolater base class).
  * Semantics follow AMReX: boxes are inclusive [lo, hi]; FArrayBox data is
  * Fortran ordered (x fastest) with component stride numPts(); coarsen uses
  * floor division.  Oracle build only. */
@@ -30,14 +31,22 @@ inline int cx_floordiv(int a, int b) {
   return a >= 0 ? a / b : -((-a + b - 1) / b);
 }
 
+struct IndexType {
+  enum CellIndex { CELL = 0, NODE = 1 };
+};
+
 struct Box {
   IntVect lo, hi;
+  IndexType::CellIndex typ[3] = {IndexType::CELL, IndexType::CELL, IndexType::CELL};
   Box() {}
   Box(const IntVect &l, const IntVect &h) : lo(l), hi(h) {}
   const int *loVect() const { return lo.v; }
   const int *hiVect() const { return hi.v; }
   const IntVect &smallEnd() const { return lo; }
   const IntVect &bigEnd() const { return hi; }
+  int smallEnd(int d) const { return lo[d]; }
+  int bigEnd(int d) const { return hi[d]; }
+  IndexType::CellIndex type(int d) const { return typ[d]; }
   bool ok() const { return lo[0] <= hi[0] && lo[1] <= hi[1] && lo[2] <= hi[2]; }
   long numPts() const {
     return ok() ? long(hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) *
@@ -87,9 +96,18 @@ struct FArrayBox {
   const Box &box() const { return bx; }
   const double *dataPtr(int c = 0) const { return ptr + c * bx.numPts(); }
   double *dataPtr(int c = 0) { return ptr + c * bx.numPts(); }
+  int nComp() const { return ncomp; }
 };
 struct IArrayBox {};
-struct Geometry {};
+// The level's cell-centred domain box and its physical extent.
+struct Geometry {
+  Box domain;
+  double problo[3] = {0, 0, 0}, probhi[3] = {1, 1, 1}, dx[3] = {1, 1, 1};
+  const Box &Domain() const { return domain; }
+  double ProbLo(int d) const { return problo[d]; }
+  double ProbHi(int d) const { return probhi[d]; }
+  double CellSize(int d) const { return dx[d]; }
+};
 struct BCRec {};
 
 template <typename F> void ParallelFor(const Box &b, const F &f) {
