@@ -32,6 +32,12 @@ One step = prolongation of every box and component of the level.  Reported:
              128^3, 8 variables): time, GB/s and fraction of the HBM peak
   limited    ENO order 3 and minmod (CCC, 64 boxes of 64^3 coarse cells, 5
              variables) as level plans: fine points/s
+  boundary   outer boundary conditions of a level (the step after a
+             prolongation): a 256^3-cell domain in 512 FABs of 32^3 cells, 3
+             ghosts, 16 variables, reflection / Dirichlet / linear
+             extrapolation / Robin / Neumann faces; one plan launch per step
+             (L2 flushed between steps), one launch per FAB beside it, and the
+             reference's BoundaryCondition on the host over the same FABs
   cpu_baseline  the reference operators compiled for the host
              (oracle/_ref, all host threads, OpenMP over boxes) on one
              component of every box
@@ -80,6 +86,8 @@ def parse():
                    help="passes of the restriction leg (0: skip)")
     p.add_argument("--limited-steps", type=int, default=2,
                    help="passes of the ENO / minmod leg (0: skip)")
+    p.add_argument("--boundary-steps", type=int, default=5,
+                   help="executions of the boundary-condition leg (0: skip)")
     p.add_argument("--boxes", type=int, default=512, help="level512: number of boxes")
     p.add_argument("--ncomp", type=int, default=24, help="level512: variables per box")
     return p.parse_args()
@@ -254,6 +262,83 @@ def limited_leg(args, cb, torch, dev, max_over_ranks, barrier):
         out[f"{typ}_pts_per_s"] = out["fine_points"] / (ms / 1e3)
         plan.close()
         del boxes
+    return out
+
+
+def boundary_leg(args, cb, torch, dev, max_over_ranks, barrier, peak):
+    """Outer boundary conditions of the level of
+    carpetx_b200.workloads.BC_LEVEL_FACES (cx_boundary_plan_*): the whole
+    outer shell, 262^3 - 256^3 points x 16 variables, per step one launch.
+    Algorithmic bytes: 8 written per value, plus 8 read unless Dirichlet.  The
+    L2 is flushed (a 256 MiB write) before each timed execution."""
+    from carpetx_b200.workloads import BC_LEVEL_FACES, boundary_spec, tiled_level_fabs
+    nc, n, g = 16, 256, 3
+    spec = boundary_spec(np.random.default_rng(args.seed + 5), nc, (1, 1, 1), (n,) * 3,
+                         nghost=g, faces=BC_LEVEL_FACES)
+    fabs = tiled_level_fabs((n,) * 3, (32,) * 3, (1, 1, 1), g)
+    side = 32 + 2 * g
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(args.seed + 5)
+    slab = torch.empty((len(fabs), nc, side, side, side), dtype=torch.float64, device=dev)
+    slab.uniform_(-1, 1, generator=gen)
+    plan = cb.BoundaryPlan(spec, [(slab[i], lo, hi) for i, (lo, hi) in enumerate(fabs)])
+    st = plan.stats()
+    flush = torch.empty(256 * 2**20 // 8, dtype=torch.float64, device=dev)
+    # FABs that reach outside the domain: the reference builds a
+    # BoundaryCondition for these only (driver.cxx:991-994)
+    edge = [i for i, (lo, hi) in enumerate(fabs)
+            if any(lo[d] < 0 or hi[d] > n - 1 for d in range(3))]
+    out = {"workload": f"{len(fabs)} FABs of 32^3 cells (+{g} ghosts) tiling a {n}^3-cell "
+                       f"domain, {nc} vars, cell centred; faces x: reflection / Dirichlet, y: "
+                       "linear extrapolation / Robin, z: Neumann / linear extrapolation",
+           "points": st["points"], "values": st["points"] * nc, "bytes": st["bytes"],
+           "fabs_with_boundary": len(edge)}
+
+    def timed(fn, steps):
+        total = 0.0
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        return total / steps
+
+    for _ in range(3):
+        plan.execute()
+    barrier()
+    ms = max_over_ranks(timed(plan.execute, args.boundary_steps))
+    gbs = st["bytes"] / (ms / 1e3) / 1e9
+    out.update({"ms": ms, "values_per_s": out["values"] / (ms / 1e3), "achieved_gbs": gbs,
+                "frac_of_peak": gbs / peak, "launches_per_step": 1})
+
+    def per_fab():
+        for i in edge:
+            cb.boundary_box(spec, slab[i], fabs[i][0], fabs[i][1])
+
+    per_fab()
+    barrier()
+    ms_pf = max_over_ranks(timed(per_fab, max(1, args.boundary_steps // 2)))
+    out.update({"per_fab_ms": ms_pf, "per_fab_launches": len(edge),
+                "batched_speedup": ms_pf / ms})
+    plan.close()
+    if not args.no_cpu_baseline:
+        from oracle.oracle import RefBoundary
+        if RefBoundary.available():
+            ref = RefBoundary()
+            host = [slab[i].cpu().numpy() for i in edge]
+            t0 = time.perf_counter()
+            for a, i in zip(host, edge):
+                ref.boundary(spec, a, fabs[i][0], fabs[i][1])
+            t = time.perf_counter() - t0
+            out["cpu_baseline"] = {"value": out["values"] / t, "unit": "values/s", "cores": 1,
+                                   "kind": "reference",
+                                   "sample": f"BoundaryCondition::apply on all {len(edge)} FABs "
+                                             "that reach the boundary (the whole level), one "
+                                             "pass; oracle/_ref parity build (-O2, asserts on)"}
+    del slab, flush
     return out
 
 
@@ -599,6 +684,8 @@ def main():
                    if args.restrict_steps > 0 else None)
     limited = (limited_leg(args, cb, torch, dev, max_over_ranks, barrier)
                if args.limited_steps > 0 else None)
+    boundary = (boundary_leg(args, cb, torch, dev, max_over_ranks, barrier, peak)
+                if args.boundary_steps > 0 else None)
 
     # per GPU: the ranks' mean algorithmic bytes over the slowest rank's time
     mean_bytes = sum_over_ranks(alg_bytes, dev) / world
@@ -635,6 +722,7 @@ def main():
         "adjoint": adjoint,
         "restriction": restriction,
         "limited": limited,
+        "boundary": boundary,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         lib, kind = cpu_lib()
