@@ -75,6 +75,11 @@ class CxBcFab(ctypes.Structure):
     _fields_ = [("data", _VP), ("lo", _I3), ("hi", _I3)]
 
 
+class CxFab(ctypes.Structure):
+    """cx_fab_t"""
+    _fields_ = [("data", _VP), ("lo", _I3), ("hi", _I3), ("valid_lo", _I3), ("valid_hi", _I3)]
+
+
 def bc_struct(spec):
     """cx_bc_t from a dict: symmetry, boundary ([face][dir] nested lists),
     domain_lo, domain_hi, prob_lo, prob_hi, dx, indextype, nghost (optional,
@@ -136,6 +141,15 @@ def lib():
         L.cx_boundary_plan_stats.argtypes = [_VP, ctypes.POINTER(ctypes.c_int64),
                                              ctypes.POINTER(ctypes.c_int64)]
         L.cx_boundary_plan_destroy.argtypes = [_VP]
+        L.cx_copy_plan_parallel_copy.argtypes = [ctypes.POINTER(CxFab), _I, ctypes.POINTER(CxFab),
+                                                 _I, _I, _I3, _I3, _I3, ctypes.POINTER(_VP)]
+        L.cx_copy_plan_fill_boundary.argtypes = [ctypes.POINTER(CxFab), _I, _I, _I3, _I3,
+                                                 ctypes.POINTER(_VP)]
+        L.cx_copy_plan_execute.argtypes = [_VP, _VP]
+        L.cx_copy_plan_stats.argtypes = [_VP, ctypes.POINTER(ctypes.c_int64),
+                                         ctypes.POINTER(ctypes.c_int64),
+                                         ctypes.POINTER(ctypes.c_int64)]
+        L.cx_copy_plan_destroy.argtypes = [_VP]
         _lib = L
     return _lib
 
@@ -281,6 +295,63 @@ class BoundaryPlan:
     def close(self):
         if self.handle:
             lib().cx_boundary_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class CopyPlan:
+    """cx_copy_plan_*: AMReX's FillBoundary or ParallelCopy of a level as one
+    launch.  FABs are tuples (tensor, lo, hi, valid_lo, valid_hi); the plan
+    keeps the tensors alive.  Build with CopyPlan.fill_boundary or
+    CopyPlan.parallel_copy."""
+
+    def __init__(self, handle, keep):
+        self.handle, self._keep = handle, keep
+
+    @staticmethod
+    def _fabs(fabs, ncomp):
+        arr = (CxFab * max(1, len(fabs)))()
+        for i, (t, lo, hi, vlo, vhi) in enumerate(fabs):
+            arr[i] = CxFab(_ptr(t, ncomp, lo, hi, "fab").value, _i3(lo), _i3(hi), _i3(vlo),
+                           _i3(vhi))
+        return arr
+
+    @classmethod
+    def fill_boundary(cls, fabs, ncomp, nghost, period=(0, 0, 0)):
+        fabs = list(fabs)
+        h = ctypes.c_void_p()
+        _check(lib().cx_copy_plan_fill_boundary(cls._fabs(fabs, ncomp), len(fabs), int(ncomp),
+                                                _i3(nghost), _i3(period), ctypes.byref(h)))
+        return cls(h, [f[0] for f in fabs])
+
+    @classmethod
+    def parallel_copy(cls, dst, src, ncomp, src_nghost=(0, 0, 0), dst_nghost=(0, 0, 0),
+                      period=(0, 0, 0)):
+        dst, src = list(dst), list(src)
+        h = ctypes.c_void_p()
+        _check(lib().cx_copy_plan_parallel_copy(cls._fabs(dst, ncomp), len(dst),
+                                                cls._fabs(src, ncomp), len(src), int(ncomp),
+                                                _i3(src_nghost), _i3(dst_nghost), _i3(period),
+                                                ctypes.byref(h)))
+        return cls(h, [f[0] for f in dst + src])
+
+    def execute(self, stream=None):
+        _check(lib().cx_copy_plan_execute(self.handle, _stream(stream)))
+
+    def stats(self):
+        a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().cx_copy_plan_stats(self.handle, ctypes.byref(a), ctypes.byref(b),
+                                        ctypes.byref(c)))
+        return {"points": a.value, "pieces": b.value, "bytes": c.value}
+
+    def close(self):
+        if self.handle:
+            lib().cx_copy_plan_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -306,6 +306,52 @@ int cx_boundary_plan_execute(cx_boundary_plan_t plan, cx_stream_t stream);
 int cx_boundary_plan_stats(cx_boundary_plan_t plan, int64_t *npoints, int64_t *bytes);
 int cx_boundary_plan_destroy(cx_boundary_plan_t plan);
 
+/* ---- Region copies: ParallelCopy and FillBoundary on one GPU ---------------
+ * The copies around a prolongation in CarpetX's sync (CarpetX/src/
+ * fillpatch.cxx:34-37, 63-64, 91-93, 122-124, 175, 205-207, 218-225): the
+ * same-level halo exchange (AMReX MultiFab::FillBoundary), the gather of the
+ * coarse patches and the scatter of the interpolated fine patches
+ * (MultiFab::ParallelCopy).  A copy plan holds the pieces (destination box,
+ * source FAB, periodic shift) computed once per regrid; executing it copies
+ * every piece of every FAB in one launch.  AMReX's sources are not in the
+ * reference tree: the rules below restate its documented behaviour.  Where
+ * several sources cover a destination point (valid boxes that share a face
+ * in vertex-centred directions, or grown source boxes), the first in list
+ * order, then image order, sets it, so that pieces never overlap.  FABs
+ * must not overlap in memory. */
+typedef struct {
+  double *data;                 /* device data, ncomp components on [lo, hi] */
+  int lo[3], hi[3];             /* the FAB: its valid box grown by its ghosts */
+  int valid_lo[3], valid_hi[3]; /* the valid box */
+} cx_fab_t;
+
+typedef struct cx_copy_plan *cx_copy_plan_t;
+
+/* dst.ParallelCopy(src, 0, 0, ncomp, src_nghost, dst_nghost, period): every
+ * point of each destination FAB's valid box grown by dst_nghost (clipped to
+ * the FAB) is set from the first source FAB whose valid box grown by
+ * src_nghost (clipped to that FAB), shifted by a periodic image (shift 0
+ * first, then -period, +period per direction, z outermost), contains it;
+ * points no source covers are left unchanged.  period[d] = 0: not periodic
+ * in d. */
+int cx_copy_plan_parallel_copy(const cx_fab_t *dst, int ndst, const cx_fab_t *src, int nsrc,
+                               int ncomp, const int src_nghost[3], const int dst_nghost[3],
+                               const int period[3], cx_copy_plan_t *out);
+
+/* mf.FillBoundary(0, ncomp, nghost, period): every point of each FAB within
+ * nghost of its valid box (clipped to the FAB) and outside it is set from
+ * the first FAB, in list order and then image order, whose valid box
+ * shifted by a periodic image contains it; a FAB is never its own source at
+ * shift 0. */
+int cx_copy_plan_fill_boundary(const cx_fab_t *fabs, int nfabs, int ncomp, const int nghost[3],
+                               const int period[3], cx_copy_plan_t *out);
+
+int cx_copy_plan_execute(cx_copy_plan_t plan, cx_stream_t stream);
+/* Points copied per execution (each ncomp values), pieces, and algorithmic
+ * bytes (16 per value: one read, one write). */
+int cx_copy_plan_stats(cx_copy_plan_t plan, int64_t *npoints, int64_t *npieces, int64_t *bytes);
+int cx_copy_plan_destroy(cx_copy_plan_t plan);
+
 #ifdef __cplusplus
 }
 #endif
