@@ -32,6 +32,9 @@ One step = prolongation of every box and component of the level.  Reported:
              128^3, 8 variables): time, GB/s and fraction of the HBM peak
   limited    ENO order 3 and minmod (CCC, 64 boxes of 64^3 coarse cells, 5
              variables) as level plans: fine points/s
+  halo       same-level halo exchange (FillBoundary) of the boundary leg's
+             level: every ghost point inside the domain from its neighbour,
+             one copy-plan launch per step (L2 flushed between steps)
   boundary   outer boundary conditions of a level (the step after a
              prolongation): a 256^3-cell domain in 512 FABs of 32^3 cells, 3
              ghosts, 16 variables, reflection / Dirichlet / linear
@@ -86,6 +89,8 @@ def parse():
                    help="passes of the restriction leg (0: skip)")
     p.add_argument("--limited-steps", type=int, default=2,
                    help="passes of the ENO / minmod leg (0: skip)")
+    p.add_argument("--halo-steps", type=int, default=5,
+                   help="executions of the halo-exchange leg (0: skip)")
     p.add_argument("--boundary-steps", type=int, default=5,
                    help="executions of the boundary-condition leg (0: skip)")
     p.add_argument("--boxes", type=int, default=512, help="level512: number of boxes")
@@ -340,6 +345,48 @@ def boundary_leg(args, cb, torch, dev, max_over_ranks, barrier, peak):
                                              "pass; oracle/_ref parity build (-O2, asserts on)"}
     del slab, flush
     return out
+
+
+def halo_leg(args, cb, torch, dev, max_over_ranks, barrier, peak):
+    """FillBoundary (cx_copy_plan_fill_boundary) of a 256^3-cell domain in
+    512 FABs of 32^3 cells with 3 ghosts, 16 components, not periodic: each
+    FAB's ghost points inside the domain from its neighbours, one launch.
+    Algorithmic bytes: 16 per value (one read, one write).  The L2 is
+    flushed (a 256 MiB write) before each timed execution."""
+    from carpetx_b200.workloads import tiled_level_fabs
+    nc, n, g = 16, 256, 3
+    fabs = tiled_level_fabs((n,) * 3, (32,) * 3, (1, 1, 1), g)
+    side = 32 + 2 * g
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(args.seed + 6)
+    slab = torch.empty((len(fabs), nc, side, side, side), dtype=torch.float64, device=dev)
+    slab.uniform_(-1, 1, generator=gen)
+    plan = cb.CopyPlan.fill_boundary(
+        [(slab[i], lo, hi, tuple(v + g for v in lo), tuple(v - g for v in hi))
+         for i, (lo, hi) in enumerate(fabs)], nc, (g, g, g))
+    st = plan.stats()
+    flush = torch.empty(256 * 2**20 // 8, dtype=torch.float64, device=dev)
+    for _ in range(3):
+        plan.execute()
+    barrier()
+    total = 0.0
+    for _ in range(args.halo_steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        plan.execute()
+        e1.record()
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    ms = max_over_ranks(total / args.halo_steps)
+    gbs = st["bytes"] / (ms / 1e3) / 1e9
+    plan.close()
+    del slab, flush
+    return {"workload": f"FillBoundary: {len(fabs)} FABs of 32^3 cells (+{g} ghosts) tiling a "
+                        f"{n}^3-cell domain, {nc} vars, cell centred, not periodic; one launch",
+            "points": st["points"], "pieces": st["pieces"], "values": st["points"] * nc,
+            "bytes": st["bytes"], "ms": ms, "values_per_s": st["points"] * nc / (ms / 1e3),
+            "achieved_gbs": gbs, "frac_of_peak": gbs / peak, "launches_per_step": 1}
 
 
 class ClockSampler:
@@ -686,6 +733,8 @@ def main():
                if args.limited_steps > 0 else None)
     boundary = (boundary_leg(args, cb, torch, dev, max_over_ranks, barrier, peak)
                 if args.boundary_steps > 0 else None)
+    halo = (halo_leg(args, cb, torch, dev, max_over_ranks, barrier, peak)
+            if args.halo_steps > 0 else None)
 
     # per GPU: the ranks' mean algorithmic bytes over the slowest rank's time
     mean_bytes = sum_over_ranks(alg_bytes, dev) / world
@@ -723,6 +772,7 @@ def main():
         "restriction": restriction,
         "limited": limited,
         "boundary": boundary,
+        "halo": halo,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         lib, kind = cpu_lib()
