@@ -272,8 +272,9 @@ def limited_leg(args, cb, torch, dev, max_over_ranks, barrier):
 
 def boundary_leg(args, cb, torch, dev, max_over_ranks, barrier, peak):
     """Outer boundary conditions of the level of
-    carpetx_b200.workloads.BC_LEVEL_FACES (cx_boundary_plan_*): the whole
-    outer shell, 262^3 - 256^3 points x 16 variables, per step one launch.
+    carpetx_b200.workloads.BC_LEVEL_FACES (cx_boundary_plan_*): every FAB's
+    points outside the domain (1.63 M: neighbouring FABs' ghosts overlap along
+    the domain's edges) x 16 variables, per step one launch.
     Algorithmic bytes: 8 written per value, plus 8 read unless Dirichlet.  The
     L2 is flushed (a 256 MiB write) before each timed execution."""
     from carpetx_b200.workloads import BC_LEVEL_FACES, boundary_spec, tiled_level_fabs
