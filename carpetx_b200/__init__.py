@@ -75,6 +75,13 @@ class CxBcFab(ctypes.Structure):
     _fields_ = [("data", _VP), ("lo", _I3), ("hi", _I3)]
 
 
+class CxRestrictBox(ctypes.Structure):
+    """cx_restrict_box_t"""
+    _fields_ = [("indextype", _I), ("ncomp", _I), ("fine", _VP), ("fine_lo", _I3),
+                ("fine_hi", _I3), ("crse", _VP), ("crse_lo", _I3), ("crse_hi", _I3),
+                ("reg_lo", _I3), ("reg_hi", _I3)]
+
+
 class CxFab(ctypes.Structure):
     """cx_fab_t"""
     _fields_ = [("data", _VP), ("lo", _I3), ("hi", _I3), ("valid_lo", _I3), ("valid_hi", _I3)]
@@ -150,6 +157,12 @@ def lib():
                                          ctypes.POINTER(ctypes.c_int64),
                                          ctypes.POINTER(ctypes.c_int64)]
         L.cx_copy_plan_destroy.argtypes = [_VP]
+        L.cx_restrict_plan_create.argtypes = [ctypes.POINTER(CxRestrictBox), _I,
+                                              ctypes.POINTER(_VP)]
+        L.cx_restrict_plan_execute.argtypes = [_VP, _VP]
+        L.cx_restrict_plan_stats.argtypes = [_VP, ctypes.POINTER(ctypes.c_int64),
+                                             ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(_I)]
+        L.cx_restrict_plan_destroy.argtypes = [_VP]
         _lib = L
     return _lib
 
@@ -295,6 +308,50 @@ class BoundaryPlan:
     def close(self):
         if self.handle:
             lib().cx_boundary_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RestrictPlan:
+    """cx_restrict_plan_*: the restriction of a whole level (every FAB pair,
+    all components) in one launch per index type.  boxes: dicts with keys
+    indextype, ncomp, fine, fine_lo, fine_hi, crse, crse_lo, crse_hi, reg_lo,
+    reg_hi (tensors as for restrict_box); the plan keeps the tensors alive."""
+
+    def __init__(self, boxes):
+        boxes = list(boxes)
+        arr = (CxRestrictBox * max(1, len(boxes)))()
+        self._keep = []
+        for i, b in enumerate(boxes):
+            n = int(b["ncomp"])
+            arr[i] = CxRestrictBox(int(b["indextype"]), n,
+                                   _ptr(b["fine"], n, b["fine_lo"], b["fine_hi"], "fine").value,
+                                   _i3(b["fine_lo"]), _i3(b["fine_hi"]),
+                                   _ptr(b["crse"], n, b["crse_lo"], b["crse_hi"], "crse").value,
+                                   _i3(b["crse_lo"]), _i3(b["crse_hi"]), _i3(b["reg_lo"]),
+                                   _i3(b["reg_hi"]))
+            self._keep += [b["fine"], b["crse"]]
+        h = ctypes.c_void_p()
+        _check(lib().cx_restrict_plan_create(arr, len(boxes), ctypes.byref(h)))
+        self.handle = h
+
+    def execute(self, stream=None):
+        _check(lib().cx_restrict_plan_execute(self.handle, _stream(stream)))
+
+    def stats(self):
+        a, b, n = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int()
+        _check(lib().cx_restrict_plan_stats(self.handle, ctypes.byref(a), ctypes.byref(b),
+                                            ctypes.byref(n)))
+        return {"coarse_values": a.value, "bytes": b.value, "launches": n.value}
+
+    def close(self):
+        if self.handle:
+            lib().cx_restrict_plan_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -618,9 +618,14 @@ int cx_level_plan_destroy(cx_level_plan_t p) {
   return CX_OK;
 }
 
-int cx_restrict_box(int indextype, const double *fine, const int fine_lo[3], const int fine_hi[3],
-                    double *crse, const int crse_lo[3], const int crse_hi[3], const int reg_lo[3],
-                    const int reg_hi[3], int ncomp, cx_stream_t stream) {
+} // extern "C"
+
+namespace {
+// The checks of cx_restrict_box; *empty: nothing to do.
+int check_restrict(int indextype, const double *fine, const int fine_lo[3], const int fine_hi[3],
+                   const double *crse, const int crse_lo[3], const int crse_hi[3],
+                   const int reg_lo[3], const int reg_hi[3], int ncomp, bool *empty) {
+  *empty = true;
   if (indextype < 0 || indextype > 7)
     return fail(CX_EUNSUPPORTED, "indextype %d out of range 0..7", indextype);
   if (!fine_lo || !fine_hi || !crse_lo || !crse_hi || !reg_lo || !reg_hi || ncomp < 0)
@@ -637,11 +642,117 @@ int cx_restrict_box(int indextype, const double *fine, const int fine_lo[3], con
       return fail(CX_EINVAL, "fine box does not contain the children of the region in direction %d",
                   d);
   }
+  *empty = false;
+  return CX_OK;
+}
+} // namespace
+
+struct cx_restrict_plan {
+  void *d_items[8] = {};
+  int nitems[8] = {};
+  int64_t npts[8] = {};
+  int64_t ncoarse = 0, bytes = 0;
+  int nlaunch = 0;
+};
+
+extern "C" {
+
+int cx_restrict_box(int indextype, const double *fine, const int fine_lo[3], const int fine_hi[3],
+                    double *crse, const int crse_lo[3], const int crse_hi[3], const int reg_lo[3],
+                    const int reg_hi[3], int ncomp, cx_stream_t stream) {
+  bool empty;
+  if (int e = check_restrict(indextype, fine, fine_lo, fine_hi, crse, crse_lo, crse_hi, reg_lo,
+                             reg_hi, ncomp, &empty))
+    return e;
+  if (empty)
+    return CX_OK;
   if (int e = check_device())
     return e;
   return cuda_status(launch_restrict_box(indextype, fine, fine_lo, fine_hi, crse, crse_lo, crse_hi,
                                          reg_lo, reg_hi, ncomp, (cudaStream_t)stream),
                      "restriction launch");
+}
+
+int cx_restrict_plan_create(const cx_restrict_box_t *boxes, int nboxes, cx_restrict_plan_t *out) {
+  if (!out || nboxes < 0 || (nboxes > 0 && !boxes))
+    return fail(CX_EINVAL, "invalid argument");
+  *out = nullptr;
+  std::vector<int> ids[8];
+  for (int i = 0; i < nboxes; ++i) {
+    const cx_restrict_box_t &b = boxes[i];
+    bool empty;
+    if (int e = check_restrict(b.indextype, b.fine, b.fine_lo, b.fine_hi, b.crse, b.crse_lo,
+                               b.crse_hi, b.reg_lo, b.reg_hi, b.ncomp, &empty))
+      return fail(e, "box %d: %s", i, g_last_error.c_str());
+    if (!empty)
+      ids[b.indextype].push_back(i);
+  }
+  if (int e = check_device())
+    return e;
+  cx_restrict_plan *p = new cx_restrict_plan;
+  const int64_t isz = restrict_item_bytes();
+  for (int it = 0; it < 8; ++it) {
+    if (ids[it].empty())
+      continue;
+    std::vector<char> buf(ids[it].size() * isz);
+    int64_t start = 0;
+    const int nch = (1 + ((it >> 2) & 1)) * (1 + ((it >> 1) & 1)) * (1 + (it & 1));
+    for (size_t n = 0; n < ids[it].size(); ++n) {
+      const cx_restrict_box_t &b = boxes[ids[it][n]];
+      const int64_t pts = restrict_fill_item(buf.data(), (int)n, b.fine, b.fine_lo, b.fine_hi,
+                                             b.crse, b.crse_lo, b.crse_hi, b.reg_lo, b.reg_hi,
+                                             b.ncomp, start);
+      start += pts;
+      p->bytes += 8 * pts * (nch + 1);
+    }
+    p->ncoarse += start;
+    p->npts[it] = start;
+    p->nitems[it] = (int)ids[it].size();
+    ++p->nlaunch;
+    cudaError_t e = cudaMalloc(&p->d_items[it], buf.size());
+    if (e == cudaSuccess)
+      e = cudaMemcpy(p->d_items[it], buf.data(), buf.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      cx_restrict_plan_destroy(p);
+      return cuda_status(e, "restriction plan upload");
+    }
+  }
+  *out = p;
+  return CX_OK;
+}
+
+int cx_restrict_plan_execute(cx_restrict_plan_t p, cx_stream_t stream) {
+  if (!p)
+    return fail(CX_EINVAL, "null plan");
+  for (int it = 0; it < 8; ++it)
+    if (p->nitems[it])
+      if (int e = cuda_status(launch_restrict_level(it, p->d_items[it], p->nitems[it],
+                                                    p->npts[it], (cudaStream_t)stream),
+                              "restriction launch"))
+        return e;
+  return CX_OK;
+}
+
+int cx_restrict_plan_stats(cx_restrict_plan_t p, int64_t *ncoarse, int64_t *bytes,
+                           int *nlaunches) {
+  if (!p)
+    return fail(CX_EINVAL, "null plan");
+  if (ncoarse)
+    *ncoarse = p->ncoarse;
+  if (bytes)
+    *bytes = p->bytes;
+  if (nlaunches)
+    *nlaunches = p->nlaunch;
+  return CX_OK;
+}
+
+int cx_restrict_plan_destroy(cx_restrict_plan_t p) {
+  if (!p)
+    return CX_OK;
+  for (void *d : p->d_items)
+    cudaFree(d);
+  delete p;
+  return CX_OK;
 }
 
 int cx_restrict_adjoint_box(int indextype, const double *crse_bar, const int crse_lo[3],

@@ -7,6 +7,8 @@
 // (average_down, _faces, _edges); fully vertex-centred data is injected
 // (average_down_nodal).  One thread per coarse point, consecutive threads on
 // consecutive coarse x, so a warp reads contiguous fine rows.
+#include <algorithm>
+
 #include "cx_internal.h"
 #include "cx_stencils.cuh"
 
@@ -23,16 +25,12 @@ struct RBox {
   int64_t rnp;
 };
 
-template <int IT> __global__ void __launch_bounds__(256) restrict_kernel(const RBox r) {
+// Coarse point (i, j, k) of component comp: the mean of its children (the
+// fine point 2c itself for fully vertex-centred data).
+template <int IT>
+__device__ __forceinline__ void restrict_point(const RBox &r, int comp, int i, int j, int k) {
   constexpr int CX = (IT >> 2) & 1, CY = (IT >> 1) & 1, CZ = IT & 1;
   constexpr double SCALE = 1.0 / ((1 + CX) * (1 + CY) * (1 + CZ));
-  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= r.rnp)
-    return;
-  const int comp = blockIdx.y;
-  const int i = r.rlo[0] + (int)(idx % r.rnx);
-  const int j = r.rlo[1] + (int)((idx / r.rnx) % r.rny);
-  const int k = r.rlo[2] + (int)(idx / ((int64_t)r.rnx * r.rny));
   const double *f = r.src + comp * r.fnp;
   const int64_t fplane = (int64_t)r.fnx * r.fny;
   const int64_t f0 =
@@ -53,6 +51,48 @@ template <int IT> __global__ void __launch_bounds__(256) restrict_kernel(const R
   }
   r.dst[comp * r.cnp + (i - r.clo[0]) + (int64_t)r.cnx * ((j - r.clo[1]) + (int64_t)r.cny * (k - r.clo[2]))] =
       res;
+}
+
+template <int IT> __global__ void __launch_bounds__(256) restrict_kernel(const RBox r) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= r.rnp)
+    return;
+  const int i = r.rlo[0] + (int)(idx % r.rnx);
+  const int j = r.rlo[1] + (int)((idx / r.rnx) % r.rny);
+  const int k = r.rlo[2] + (int)(idx / ((int64_t)r.rnx * r.rny));
+  restrict_point<IT>(r, blockIdx.y, i, j, k);
+}
+
+// A level's boxes of one index type: a flat range over (box, component,
+// region point), boxes found by binary search on their first point.
+struct RItem {
+  RBox r;
+  int64_t start; // first point of the box in the launch's range
+  int ncomp;
+};
+
+template <int IT>
+__global__ void __launch_bounds__(256)
+    restrict_level_kernel(const RItem *__restrict__ items, int nitems, int64_t npts) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npts; p += stride) {
+    int a = 0, b = nitems - 1;
+    while (a < b) {
+      const int m = (a + b + 1) >> 1;
+      if (items[m].start <= p)
+        a = m;
+      else
+        b = m - 1;
+    }
+    const RBox &r = items[a].r;
+    const int64_t l = p - items[a].start;
+    const int comp = (int)(l / r.rnp);
+    const int64_t idx = l - comp * r.rnp;
+    const int i = r.rlo[0] + (int)(idx % r.rnx);
+    const int j = r.rlo[1] + (int)((idx / r.rnx) % r.rny);
+    const int k = r.rlo[2] + (int)(idx / ((int64_t)r.rnx * r.rny));
+    restrict_point<IT>(r, comp, i, j, k);
+  }
 }
 
 // Transpose: every child receives the coarse cotangent times the scale (the
@@ -134,7 +174,41 @@ template <int IT> struct AdjLaunch {
   }
 };
 
+template <int IT> struct LevelLaunch {
+  static cudaError_t go(const void *items, int nitems, int64_t npts, cudaStream_t s) {
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t want = (npts + 255) / 256;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)nsm * 8));
+    restrict_level_kernel<IT><<<grid, 256, 0, s>>>((const RItem *)items, nitems, npts);
+    return cudaGetLastError();
+  }
+};
+
 } // namespace
+
+// Restriction level plans: the boxes grouped by index type, one device item
+// list per group, one launch per group.
+int64_t restrict_item_bytes() { return (int64_t)sizeof(RItem); }
+
+// Fills item n of a host buffer of RItem; returns the box's points x ncomp.
+int64_t restrict_fill_item(void *buf, int n, const double *fine, const int flo[3],
+                           const int fhi[3], double *crse, const int clo[3], const int chi[3],
+                           const int rlo[3], const int rhi[3], int ncomp, int64_t start) {
+  RItem &it = ((RItem *)buf)[n];
+  it.r = make_rbox(fine, crse, flo, fhi, clo, chi, rlo, rhi);
+  it.start = start;
+  it.ncomp = ncomp;
+  return it.r.rnp * ncomp;
+}
+
+cudaError_t launch_restrict_level(int indextype, const void *d_items, int nitems, int64_t npts,
+                                  cudaStream_t s) {
+  if (nitems <= 0 || npts <= 0)
+    return cudaSuccess;
+  return by_indextype<LevelLaunch>(indextype, d_items, nitems, npts, s);
+}
 
 cudaError_t launch_restrict_box(int indextype, const double *fine, const int flo[3], const int fhi[3],
                                 double *crse, const int clo[3], const int chi[3], const int rlo[3],

@@ -202,6 +202,31 @@ int cx_restrict_box(int indextype, const double *fine, const int fine_lo[3],
                     const int crse_hi[3], const int reg_lo[3],
                     const int reg_hi[3], int ncomp, cx_stream_t stream);
 
+/* The restriction of a whole level: average_down of every FAB pair of a
+ * MultiFab (schedule.cxx:2793-2815 calls it once per level and group; AMReX
+ * loops over the FABs), with the arithmetic of cx_restrict_box.  The plan
+ * holds a device list of the boxes; executing it launches once per index
+ * type present (one for a group).  Validation as cx_restrict_box, per box;
+ * boxes with an empty region are skipped.  Coarse regions of distinct boxes
+ * must not overlap. */
+typedef struct {
+  int indextype, ncomp;
+  const double *fine;
+  int fine_lo[3], fine_hi[3];
+  double *crse;
+  int crse_lo[3], crse_hi[3];
+  int reg_lo[3], reg_hi[3];
+} cx_restrict_box_t;
+typedef struct cx_restrict_plan *cx_restrict_plan_t;
+int cx_restrict_plan_create(const cx_restrict_box_t *boxes, int nboxes,
+                            cx_restrict_plan_t *out);
+int cx_restrict_plan_execute(cx_restrict_plan_t plan, cx_stream_t stream);
+/* Coarse values set per execution, algorithmic bytes (8 per child read, 8
+ * per coarse value written) and launches per execution. */
+int cx_restrict_plan_stats(cx_restrict_plan_t plan, int64_t *ncoarse, int64_t *bytes,
+                           int *nlaunches);
+int cx_restrict_plan_destroy(cx_restrict_plan_t plan);
+
 /* ---------------------------------------------------------------------- */
 /* Adjoints (no reference counterpart: the transposes of the above)        */
 
