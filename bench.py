@@ -223,9 +223,52 @@ def restrict_leg(args, cb, torch, dev, max_over_ranks, barrier, peak):
     ms = max_over_ranks(e0.elapsed_time(e1)) / args.restrict_steps
     gbs = nbytes / (ms / 1e3) / 1e9
     del f, c
-    return {"workload": "restriction CCC (average_down), fine 256^3 -> coarse 128^3, 8 vars, "
-                        "one launch", "ms": ms, "bytes": nbytes, "achieved_gbs": gbs,
-            "frac_of_peak": gbs / peak}
+    out = {"workload": "restriction CCC (average_down), fine 256^3 -> coarse 128^3, 8 vars, "
+                       "one launch", "ms": ms, "bytes": nbytes, "achieved_gbs": gbs,
+           "frac_of_peak": gbs / peak}
+    # the whole mixed level (the prolongation's 512 boxes, four centrings, 8
+    # vars) restricted by one plan (one launch per index type) and by one
+    # cx_restrict_box call per box
+    from carpetx_b200.workloads import mixed_level_boxes
+    boxes = []
+    for it, clo, chi, flo, fhi in mixed_level_boxes(args.seed, nboxes=512):
+        cc = [(it >> (2 - d)) & 1 for d in range(3)]
+        fine = torch.empty((nc,) + box_shape(flo, fhi), dtype=torch.float64, device=dev)
+        fine.normal_(generator=gen)
+        crse = torch.zeros((nc,) + box_shape(clo, chi), dtype=torch.float64, device=dev)
+        boxes.append(dict(indextype=it, ncomp=nc, fine=fine, fine_lo=flo, fine_hi=fhi, crse=crse,
+                          crse_lo=clo, crse_hi=chi, reg_lo=tuple(v // 2 for v in flo),
+                          reg_hi=tuple((fhi[d] - cc[d]) // 2 for d in range(3))))
+    plan = cb.RestrictPlan(boxes)
+    st = plan.stats()
+
+    def per_box():
+        for b in boxes:
+            cb.restrict_box(b["indextype"], b["fine"], b["fine_lo"], b["fine_hi"], b["crse"],
+                            b["crse_lo"], b["crse_hi"], b["reg_lo"], b["reg_hi"], nc)
+
+    res = {}
+    for name, fn in (("plan", plan.execute), ("per_box", per_box)):
+        for _ in range(3):
+            fn()
+        barrier()
+        e0.record()
+        for _ in range(args.restrict_steps):
+            fn()
+        e1.record()
+        barrier()
+        res[name] = max_over_ranks(e0.elapsed_time(e1)) / args.restrict_steps
+    lgbs = st["bytes"] / (res["plan"] / 1e3) / 1e9
+    out["level"] = {"workload": f"{len(boxes)} boxes of the mixed level (VVV, CCC, VVC, VCC), "
+                                f"{nc} vars; inputs {sum(b['fine'].numel() for b in boxes) * 8 / 1e9:.1f}"
+                                " GB > L2, no flush",
+                    "ms": res["plan"], "launches": st["launches"], "bytes": st["bytes"],
+                    "achieved_gbs": lgbs, "frac_of_peak": lgbs / peak,
+                    "per_box_ms": res["per_box"], "per_box_launches": len(boxes),
+                    "batched_speedup": res["per_box"] / res["plan"]}
+    plan.close()
+    del boxes
+    return out
 
 
 def limited_leg(args, cb, torch, dev, max_over_ranks, barrier):
