@@ -102,28 +102,41 @@ __host__ __device__ __forceinline__ Access access_of(const Region &g, const int 
   return a;
 }
 
-// regs: the level plan's device list, or nullptr for the regions passed by
-// value (one FAB).
+// regs: the level plan's device list, with first[c] the region containing
+// point c * kThreads (a thread scans forward from it); or nullptr for the
+// regions passed by value (one FAB, at most 26: binary search).  Offsets
+// within a region fit in 32 bits (checked on the host).
 __global__ void __launch_bounds__(kThreads)
     boundary_kernel(const __grid_constant__ Consts k, const Region *__restrict__ regs,
-                    const __grid_constant__ BoxRegions own) {
+                    const int *__restrict__ first, const __grid_constant__ BoxRegions own) {
   const Region *R = regs ? regs : own.r;
-  const int64_t stride = (int64_t)gridDim.x * kThreads;
-  for (int64_t p = (int64_t)blockIdx.x * kThreads + threadIdx.x; p < k.npts; p += stride) {
-    int a = 0, b = k.nreg - 1; // last region starting at or before p
-    while (a < b) {
-      const int m = (a + b + 1) >> 1;
-      if (R[m].start <= p)
-        a = m;
-      else
-        b = m - 1;
+  const int64_t nchunks = (k.npts + kThreads - 1) / kThreads;
+  for (int64_t chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+    const int64_t p = chunk * kThreads + threadIdx.x;
+    if (p >= k.npts)
+      continue;
+    int a;
+    if (regs) {
+      a = first[chunk];
+      while (a + 1 < k.nreg && R[a + 1].start <= p)
+        ++a;
+    } else {
+      a = 0; // last region starting at or before p
+      int b = k.nreg - 1;
+      while (a < b) {
+        const int m = (a + b + 1) >> 1;
+        if (R[m].start <= p)
+          a = m;
+        else
+          b = m - 1;
+      }
     }
     const Region &g = R[a];
-    int64_t l = p - g.start;
-    const int i = (int)(l % g.ext[0]);
-    l /= g.ext[0];
-    const int j = (int)(l % g.ext[1]);
-    const int kz = (int)(l / g.ext[1]);
+    const int l = (int)(p - g.start);
+    const int i = l % g.ext[0];
+    const int jk = l / g.ext[0];
+    const int j = jk % g.ext[1];
+    const int kz = jk / g.ext[1];
     const int dst[3] = {g.bmin[0] + i, g.bmin[1] + j, g.bmin[2] + kz};
     const Access x = access_of(g, dst);
     // Robin: the fall-off factor |x_src| / |x_dst| is the same in every
@@ -340,6 +353,8 @@ int add_fab(const cx_bc_t &bc, double *data, const int lo[3], const int hi[3],
         if (!region_in_fab(g))
           return bad("internal error: a region's access leaves its FAB");
         const int64_t n = (int64_t)g.ext[0] * g.ext[1] * g.ext[2];
+        if (n > INT32_MAX)
+          return bad("a region of more than 2^31 points");
         g.start = npts;
         npts += n;
         bytes += n * bc.ncomp * ((g.flags & F_DIRICHLET) ? 8 : 16);
@@ -356,10 +371,11 @@ int grid_for(int64_t npts) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)nsm * 8));
 }
 
-int launch(const Consts &k, const Region *d_regs, const BoxRegions &own, cudaStream_t s) {
+int launch(const Consts &k, const Region *d_regs, const int *d_first, const BoxRegions &own,
+           cudaStream_t s) {
   if (k.npts == 0)
     return CX_OK;
-  boundary_kernel<<<grid_for(k.npts), kThreads, 0, s>>>(k, d_regs, own);
+  boundary_kernel<<<grid_for(k.npts), kThreads, 0, s>>>(k, d_regs, d_first, own);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     char buf[256];
@@ -381,6 +397,7 @@ bool all_periodic(const cx_bc_t &bc) {
 struct cx_boundary_plan {
   Consts k{};
   Region *d_regs = nullptr;
+  int *d_first = nullptr; // chunk of kThreads points -> its first region
   int64_t bytes = 0;
 };
 
@@ -399,7 +416,7 @@ int cx_boundary_box(const cx_bc_t *bc, double *data, const int lo[3], const int 
   std::copy(regs.begin(), regs.end(), own.r);
   k.nreg = (int)regs.size();
   k.npts = npts;
-  return launch(k, nullptr, own, (cudaStream_t)stream);
+  return launch(k, nullptr, nullptr, own, (cudaStream_t)stream);
 }
 
 int cx_boundary_plan_create(const cx_bc_t *bc, const cx_bc_fab_t *fabs, int nfabs,
@@ -444,11 +461,23 @@ int cx_boundary_plan_create(const cx_bc_t *bc, const cx_bc_fab_t *fabs, int nfab
   p->k.npts = npts;
   p->bytes = bytes;
   if (!regs.empty()) {
+    std::vector<int> first((npts + kThreads - 1) / kThreads);
+    size_t a = 0;
+    for (size_t c = 0; c < first.size(); ++c) {
+      while (a + 1 < regs.size() && regs[a + 1].start <= (int64_t)c * kThreads)
+        ++a;
+      first[c] = (int)a;
+    }
     cudaError_t e = cudaMalloc(&p->d_regs, regs.size() * sizeof(Region));
     if (e == cudaSuccess)
       e = cudaMemcpy(p->d_regs, regs.data(), regs.size() * sizeof(Region), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMalloc(&p->d_first, first.size() * sizeof(int));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(p->d_first, first.data(), first.size() * sizeof(int), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
       cudaFree(p->d_regs);
+      cudaFree(p->d_first);
       delete p;
       char buf[256];
       snprintf(buf, sizeof buf, "boundary plan upload: %s", cudaGetErrorString(e));
@@ -463,7 +492,7 @@ int cx_boundary_plan_execute(cx_boundary_plan_t p, cx_stream_t stream) {
   if (!p)
     return bad("null plan");
   static const BoxRegions none{};
-  return launch(p->k, p->d_regs, none, (cudaStream_t)stream);
+  return launch(p->k, p->d_regs, p->d_first, none, (cudaStream_t)stream);
 }
 
 int cx_boundary_plan_stats(cx_boundary_plan_t p, int64_t *npoints, int64_t *bytes) {
@@ -480,6 +509,7 @@ int cx_boundary_plan_destroy(cx_boundary_plan_t p) {
   if (!p)
     return CX_OK;
   cudaFree(p->d_regs);
+  cudaFree(p->d_first);
   delete p;
   return CX_OK;
 }

@@ -649,6 +649,7 @@ int check_restrict(int indextype, const double *fine, const int fine_lo[3], cons
 
 struct cx_restrict_plan {
   void *d_items[8] = {};
+  int *d_first[8] = {}; // per chunk of 256 points: its first item
   int nitems[8] = {};
   int64_t npts[8] = {};
   int64_t ncoarse = 0, bytes = 0;
@@ -695,6 +696,7 @@ int cx_restrict_plan_create(const cx_restrict_box_t *boxes, int nboxes, cx_restr
     if (ids[it].empty())
       continue;
     std::vector<char> buf(ids[it].size() * isz);
+    std::vector<int64_t> starts(ids[it].size());
     int64_t start = 0;
     const int nch = (1 + ((it >> 2) & 1)) * (1 + ((it >> 1) & 1)) * (1 + (it & 1));
     for (size_t n = 0; n < ids[it].size(); ++n) {
@@ -702,8 +704,20 @@ int cx_restrict_plan_create(const cx_restrict_box_t *boxes, int nboxes, cx_restr
       const int64_t pts = restrict_fill_item(buf.data(), (int)n, b.fine, b.fine_lo, b.fine_hi,
                                              b.crse, b.crse_lo, b.crse_hi, b.reg_lo, b.reg_hi,
                                              b.ncomp, start);
+      if (pts > INT32_MAX) {
+        cx_restrict_plan_destroy(p);
+        return fail(CX_EINVAL, "box %d: more than 2^31 coarse values", ids[it][n]);
+      }
+      starts[n] = start;
       start += pts;
       p->bytes += 8 * pts * (nch + 1);
+    }
+    std::vector<int> first((start + 255) / 256);
+    size_t a = 0;
+    for (size_t c = 0; c < first.size(); ++c) {
+      while (a + 1 < starts.size() && starts[a + 1] <= (int64_t)c * 256)
+        ++a;
+      first[c] = (int)a;
     }
     p->ncoarse += start;
     p->npts[it] = start;
@@ -712,6 +726,11 @@ int cx_restrict_plan_create(const cx_restrict_box_t *boxes, int nboxes, cx_restr
     cudaError_t e = cudaMalloc(&p->d_items[it], buf.size());
     if (e == cudaSuccess)
       e = cudaMemcpy(p->d_items[it], buf.data(), buf.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMalloc(&p->d_first[it], first.size() * sizeof(int));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(p->d_first[it], first.data(), first.size() * sizeof(int),
+                     cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
       cx_restrict_plan_destroy(p);
       return cuda_status(e, "restriction plan upload");
@@ -726,8 +745,9 @@ int cx_restrict_plan_execute(cx_restrict_plan_t p, cx_stream_t stream) {
     return fail(CX_EINVAL, "null plan");
   for (int it = 0; it < 8; ++it)
     if (p->nitems[it])
-      if (int e = cuda_status(launch_restrict_level(it, p->d_items[it], p->nitems[it],
-                                                    p->npts[it], (cudaStream_t)stream),
+      if (int e = cuda_status(launch_restrict_level(it, p->d_items[it], p->d_first[it],
+                                                    p->nitems[it], p->npts[it],
+                                                    (cudaStream_t)stream),
                               "restriction launch"))
         return e;
   return CX_OK;
@@ -750,6 +770,8 @@ int cx_restrict_plan_destroy(cx_restrict_plan_t p) {
   if (!p)
     return CX_OK;
   for (void *d : p->d_items)
+    cudaFree(d);
+  for (int *d : p->d_first)
     cudaFree(d);
   delete p;
   return CX_OK;

@@ -8,7 +8,8 @@
 // source wins), so the pieces of one FAB are disjoint boxes and one launch
 // over all pieces of all FABs has no write conflicts.  A piece is a box in
 // destination coordinates and a shift to its source FAB.  The kernel runs a
-// flat range over the pieces' points: a thread copies one point, all
+// flat range over the pieces' points, cut into chunks of one CTA's threads
+// whose first piece the host tabulates: a thread copies one point, all
 // components.
 #include <algorithm>
 #include <array>
@@ -45,24 +46,27 @@ __host__ __device__ __forceinline__ int64_t offset_in(const int o[3], int nx, in
   return (int64_t)(q[0] - o[0]) + nx * ((int64_t)(q[1] - o[1]) + (int64_t)ny * (q[2] - o[2]));
 }
 
+// Chunk c of kThreads consecutive points starts in piece first[c]; a thread
+// scans forward from there to the last piece starting at or before its
+// point (pieces are non-empty, so starts increase strictly).  Offsets within
+// a piece fit in 32 bits (checked on the host).
 __global__ void __launch_bounds__(kThreads)
-    copy_kernel(const Piece *__restrict__ P, int npieces, int64_t npts, int ncomp) {
-  const int64_t stride = (int64_t)gridDim.x * kThreads;
-  for (int64_t p = (int64_t)blockIdx.x * kThreads + threadIdx.x; p < npts; p += stride) {
-    int a = 0, b = npieces - 1; // last piece starting at or before p
-    while (a < b) {
-      const int m = (a + b + 1) >> 1;
-      if (P[m].start <= p)
-        a = m;
-      else
-        b = m - 1;
-    }
+    copy_kernel(const Piece *__restrict__ P, const int *__restrict__ first, int npieces,
+                int64_t npts, int ncomp) {
+  const int64_t nchunks = (npts + kThreads - 1) / kThreads;
+  for (int64_t chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+    const int64_t p = chunk * kThreads + threadIdx.x;
+    if (p >= npts)
+      continue;
+    int a = first[chunk];
+    while (a + 1 < npieces && P[a + 1].start <= p)
+      ++a;
     const Piece &g = P[a];
-    int64_t l = p - g.start;
-    const int i = (int)(l % g.ext[0]);
-    l /= g.ext[0];
-    const int j = (int)(l % g.ext[1]);
-    const int k = (int)(l / g.ext[1]);
+    const int l = (int)(p - g.start);
+    const int i = l % g.ext[0];
+    const int jk = l / g.ext[0];
+    const int j = jk % g.ext[1];
+    const int k = jk / g.ext[1];
     const int d[3] = {g.bmin[0] + i, g.bmin[1] + j, g.bmin[2] + k};
     const int s[3] = {d[0] + g.shift[0], d[1] + g.shift[1], d[2] + g.shift[2]};
     const double *src = g.src + offset_in(g.slo, g.snx, g.sny, s);
@@ -241,8 +245,24 @@ bool pieces_in_bounds(const std::vector<Piece> &ps) {
           a + g.shift[d] < g.slo[d] || b + g.shift[d] > g.slo[d] + sn[d] - 1)
         return false;
     }
+    if ((int64_t)g.ext[0] * g.ext[1] * g.ext[2] > INT32_MAX)
+      return false;
   }
   return true;
+}
+
+// first[c]: the piece containing point c * kThreads.
+std::vector<int> chunk_firsts(const std::vector<Piece> &ps, int64_t npts) {
+  const int64_t nchunks = (npts + kThreads - 1) / kThreads;
+  std::vector<int> f(nchunks);
+  size_t a = 0;
+  for (int64_t c = 0; c < nchunks; ++c) {
+    const int64_t p = c * kThreads;
+    while (a + 1 < ps.size() && ps[a + 1].start <= p)
+      ++a;
+    f[c] = (int)a;
+  }
+  return f;
 }
 
 std::vector<IBox> source_regions(const cx_fab_t *src, int n, const int ng[3]) {
@@ -274,6 +294,7 @@ int check_common(int ncomp, const int *a, const int *b, const int period[3], voi
 
 struct cx_copy_plan {
   Piece *d_pieces = nullptr;
+  int *d_first = nullptr; // chunk -> first piece
   int npieces = 0;
   int64_t npts = 0;
   int ncomp = 0;
@@ -291,12 +312,19 @@ int finish(Builder &b, int ncomp, cx_copy_plan_t *out) {
   p->npts = b.npts;
   p->ncomp = ncomp;
   if (!b.pieces.empty()) {
+    const std::vector<int> first = chunk_firsts(b.pieces, b.npts);
     cudaError_t e = cudaMalloc(&p->d_pieces, b.pieces.size() * sizeof(Piece));
     if (e == cudaSuccess)
       e = cudaMemcpy(p->d_pieces, b.pieces.data(), b.pieces.size() * sizeof(Piece),
                      cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMalloc(&p->d_first, first.size() * sizeof(int));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(p->d_first, first.data(), first.size() * sizeof(int),
+                     cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
       cudaFree(p->d_pieces);
+      cudaFree(p->d_first);
       delete p;
       char buf[256];
       snprintf(buf, sizeof buf, "copy plan upload: %s", cudaGetErrorString(e));
@@ -372,8 +400,8 @@ int cx_copy_plan_execute(cx_copy_plan_t p, cx_stream_t stream) {
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const int64_t want = (p->npts + kThreads - 1) / kThreads;
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)nsm * 8));
-  copy_kernel<<<grid, kThreads, 0, (cudaStream_t)stream>>>(p->d_pieces, p->npieces, p->npts,
-                                                           p->ncomp);
+  copy_kernel<<<grid, kThreads, 0, (cudaStream_t)stream>>>(p->d_pieces, p->d_first, p->npieces,
+                                                           p->npts, p->ncomp);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     char buf[256];
@@ -399,6 +427,7 @@ int cx_copy_plan_destroy(cx_copy_plan_t p) {
   if (!p)
     return CX_OK;
   cudaFree(p->d_pieces);
+  cudaFree(p->d_first);
   delete p;
   return CX_OK;
 }

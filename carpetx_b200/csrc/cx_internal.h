@@ -97,13 +97,13 @@ cudaError_t launch_point_level(const BoxDesc *d_boxes, const TileRef *d_tiles,
 
 // Restriction level plans (restrict.cu): size of one device item, host-side
 // fill of item n (returns its points x ncomp), one launch over the items of
-// one index type.
+// one index type (first[c]: the item containing point c * 256).
 int64_t restrict_item_bytes();
 int64_t restrict_fill_item(void *buf, int n, const double *fine, const int flo[3],
                            const int fhi[3], double *crse, const int clo[3], const int chi[3],
                            const int rlo[3], const int rhi[3], int ncomp, int64_t start);
-cudaError_t launch_restrict_level(int indextype, const void *d_items, int nitems, int64_t npts,
-                                  cudaStream_t s);
+cudaError_t launch_restrict_level(int indextype, const void *d_items, const int *d_first,
+                                  int nitems, int64_t npts, cudaStream_t s);
 cudaError_t launch_restrict_box(int indextype, const double *fine,
                                 const int flo[3], const int fhi[3],
                                 double *crse, const int clo[3],

@@ -71,26 +71,29 @@ struct RItem {
   int ncomp;
 };
 
+// first[c]: the item containing point c * 256 (a thread scans forward from
+// it).  An item's points x components fit in 32 bits (checked on the host).
 template <int IT>
 __global__ void __launch_bounds__(256)
-    restrict_level_kernel(const RItem *__restrict__ items, int nitems, int64_t npts) {
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < npts; p += stride) {
-    int a = 0, b = nitems - 1;
-    while (a < b) {
-      const int m = (a + b + 1) >> 1;
-      if (items[m].start <= p)
-        a = m;
-      else
-        b = m - 1;
-    }
+    restrict_level_kernel(const RItem *__restrict__ items, const int *__restrict__ first,
+                          int nitems, int64_t npts) {
+  const int64_t nchunks = (npts + 255) / 256;
+  for (int64_t chunk = blockIdx.x; chunk < nchunks; chunk += gridDim.x) {
+    const int64_t p = chunk * 256 + threadIdx.x;
+    if (p >= npts)
+      continue;
+    int a = first[chunk];
+    while (a + 1 < nitems && items[a + 1].start <= p)
+      ++a;
     const RBox &r = items[a].r;
-    const int64_t l = p - items[a].start;
-    const int comp = (int)(l / r.rnp);
-    const int64_t idx = l - comp * r.rnp;
-    const int i = r.rlo[0] + (int)(idx % r.rnx);
-    const int j = r.rlo[1] + (int)((idx / r.rnx) % r.rny);
-    const int k = r.rlo[2] + (int)(idx / ((int64_t)r.rnx * r.rny));
+    const int l = (int)(p - items[a].start);
+    const int rnp = (int)r.rnp;
+    const int comp = l / rnp;
+    const int idx = l - comp * rnp;
+    const int i = r.rlo[0] + idx % r.rnx;
+    const int jk = idx / r.rnx;
+    const int j = r.rlo[1] + jk % r.rny;
+    const int k = r.rlo[2] + jk / r.rny;
     restrict_point<IT>(r, comp, i, j, k);
   }
 }
@@ -175,13 +178,14 @@ template <int IT> struct AdjLaunch {
 };
 
 template <int IT> struct LevelLaunch {
-  static cudaError_t go(const void *items, int nitems, int64_t npts, cudaStream_t s) {
+  static cudaError_t go(const void *items, const int *first, int nitems, int64_t npts,
+                        cudaStream_t s) {
     int dev = 0, nsm = 148;
     if (cudaGetDevice(&dev) == cudaSuccess)
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const int64_t want = (npts + 255) / 256;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)nsm * 8));
-    restrict_level_kernel<IT><<<grid, 256, 0, s>>>((const RItem *)items, nitems, npts);
+    restrict_level_kernel<IT><<<grid, 256, 0, s>>>((const RItem *)items, first, nitems, npts);
     return cudaGetLastError();
   }
 };
@@ -203,11 +207,11 @@ int64_t restrict_fill_item(void *buf, int n, const double *fine, const int flo[3
   return it.r.rnp * ncomp;
 }
 
-cudaError_t launch_restrict_level(int indextype, const void *d_items, int nitems, int64_t npts,
-                                  cudaStream_t s) {
+cudaError_t launch_restrict_level(int indextype, const void *d_items, const int *d_first,
+                                  int nitems, int64_t npts, cudaStream_t s) {
   if (nitems <= 0 || npts <= 0)
     return cudaSuccess;
-  return by_indextype<LevelLaunch>(indextype, d_items, nitems, npts, s);
+  return by_indextype<LevelLaunch>(indextype, d_items, d_first, nitems, npts, s);
 }
 
 cudaError_t launch_restrict_box(int indextype, const double *fine, const int flo[3], const int fhi[3],
