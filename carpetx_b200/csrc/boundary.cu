@@ -154,21 +154,42 @@ __global__ void __launch_bounds__(kThreads)
       }
       s = __dsqrt_rn((double)(n2 / d2));
     }
-    double *col = g.data;
-    for (int c = 0; c < k.ncomp; ++c, col += g.np) {
-      double val;
-      if (g.flags & F_DIRICHLET) {
-        val = k.dirichlet[c];
-      } else {
-        val = col[x.os];
-        for (int r = 0; r < g.nrobin; ++r)
-          val = __dadd_rn(k.robin[c], __dmul_rn(q, __dsub_rn(val, k.robin[c])));
-        if (g.flags & F_LINEXT)
-          val = __dadd_rn(val, __dmul_rn(s, __dsub_rn(val, col[x.osp])));
-        if ((g.negpar >> c) & 1u) // parity -1 (only set in reflection regions)
-          val = -val;
+    // Components in groups of four: their source values are loaded before
+    // any of them is stored (no point read in a launch is written in it), so
+    // four loads are in flight; each component's arithmetic is unchanged.
+    const bool dir = g.flags & F_DIRICHLET, lin = g.flags & F_LINEXT;
+    for (int c0 = 0; c0 < k.ncomp; c0 += 4) {
+      const int n = min(4, k.ncomp - c0);
+      double v[4], w[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        v[u] = w[u] = 0;
+        if (u < n && !dir) {
+          const double *col = g.data + (int64_t)(c0 + u) * g.np;
+          v[u] = col[x.os];
+          if (lin)
+            w[u] = col[x.osp];
+        }
       }
-      col[x.od] = val;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (u >= n)
+          break;
+        const int c = c0 + u;
+        double val;
+        if (dir) {
+          val = k.dirichlet[c];
+        } else {
+          val = v[u];
+          for (int r = 0; r < g.nrobin; ++r)
+            val = __dadd_rn(k.robin[c], __dmul_rn(q, __dsub_rn(val, k.robin[c])));
+          if (lin)
+            val = __dadd_rn(val, __dmul_rn(s, __dsub_rn(val, w[u])));
+          if ((g.negpar >> c) & 1u) // parity -1 (only set in reflection regions)
+            val = -val;
+        }
+        g.data[(int64_t)c * g.np + x.od] = val;
+      }
     }
   }
 }
