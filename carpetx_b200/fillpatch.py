@@ -12,9 +12,11 @@ interpolates locally (:114-119).  This module is that exchange step:
   x (patch p owned by rank R) = box(c) n patch(p), a pure function of the box
   lists and owner maps, sorted so that both ends of every rank pair post
   their messages in the same order;
-- pieces with S == R are copied locally; the others are packed by S, sent
-  point to point (torch.distributed batched isend/irecv: NCCL over NVLink
-  between GPUs, gloo between CPU processes) and unpacked by R.
+- pieces with S == R are copied locally: on CUDA tensors all of them in one
+  launch of a copy plan (cx_copy_plan_parallel_copy), elsewhere one tensor
+  copy each; the others are packed by S, sent point to point
+  (torch.distributed batched isend/irecv: NCCL over NVLink between GPUs,
+  gloo between CPU processes) and unpacked by R.
 
 Patch points that no coarse box covers (outside the coarse level) are left as
 they are, as ParallelCopy leaves them; boundary conditions fill them.
@@ -71,6 +73,8 @@ class CoarsePatchExchange:
         self.patch_boxes = [tuple(map(tuple, b)) for b in patch_boxes]
         self.rank = rank
         self.pieces = patch_pieces(self.coarse_boxes, coarse_owner, self.patch_boxes, patch_owner)
+        self._plan = None
+        self._plan_key = None
 
     def stats(self) -> Dict[str, int]:
         """Points this rank sends, receives and copies locally (per component)."""
@@ -95,10 +99,16 @@ class CoarsePatchExchange:
         import torch.distributed as dist
         ops: List = []
         recvs = []
+        local = [(ci, pi, piece) for src, dst, ci, pi, piece in self.pieces
+                 if src == self.rank and dst == self.rank]
+        plan = self._local_plan(local, coarse_data, patch_data)
+        if plan is not None:
+            plan.execute()
         for src, dst, ci, pi, piece in self.pieces:
             if src == self.rank and dst == self.rank:
-                _view(patch_data[pi], self.patch_boxes[pi], piece).copy_(
-                    _view(coarse_data[ci], self.coarse_boxes[ci], piece))
+                if plan is None:
+                    _view(patch_data[pi], self.patch_boxes[pi], piece).copy_(
+                        _view(coarse_data[ci], self.coarse_boxes[ci], piece))
             elif src == self.rank:
                 buf = _view(coarse_data[ci], self.coarse_boxes[ci], piece).contiguous()
                 ops.append(dist.P2POp(dist.isend, buf, dst))
@@ -113,3 +123,31 @@ class CoarsePatchExchange:
                 req.wait()
         for pi, piece, buf in recvs:
             _view(patch_data[pi], self.patch_boxes[pi], piece).copy_(buf)
+
+    def _local_plan(self, local, coarse_data, patch_data):
+        """A copy plan for the local pieces when every tensor they involve is
+        a CUDA float64 tensor (None otherwise), rebuilt when a tensor
+        changes.  The pieces are applied in list order, so where coarse boxes
+        overlap (shared vertex faces) the last one sets a point; the plan's
+        first source wins, so it gets the coarse boxes in reverse order."""
+        if not local:
+            return None
+        cis = sorted({ci for ci, _, _ in local}, reverse=True)
+        pis = sorted({pi for _, pi, _ in local})
+        ts = [coarse_data[ci] for ci in cis] + [patch_data[pi] for pi in pis]
+        if not all(getattr(t, "is_cuda", False) and str(t.dtype) == "torch.float64"
+                   for t in ts):
+            return None
+        key = tuple(t.data_ptr() for t in ts)
+        if key != self._plan_key:
+            from carpetx_b200 import CopyPlan
+            ncomp = int(ts[0].shape[0])
+            src = [(coarse_data[ci],) + self.coarse_boxes[ci] + self.coarse_boxes[ci]
+                   for ci in cis]
+            dst = [(patch_data[pi],) + self.patch_boxes[pi] + self.patch_boxes[pi]
+                   for pi in pis]
+            if self._plan is not None:
+                self._plan.close()
+            self._plan = CopyPlan.parallel_copy(dst, src, ncomp)
+            self._plan_key = key
+        return self._plan

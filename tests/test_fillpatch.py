@@ -149,3 +149,29 @@ def _rank_main(rank, world, port):
 def test_two_gloo_ranks_gather_coarse_patches(world):
     mp.start_processes(_rank_main, args=(world, _free_port()), nprocs=world, join=True,
                        start_method="spawn")
+
+
+@pytest.mark.gpu
+def test_gpu_exchange_local_copy_plan_matches_tensor_copies(dev):
+    """One rank owning everything: the local pieces go through one copy-plan
+    launch on CUDA tensors and through one tensor copy each on CPU tensors;
+    vertex-centred coarse boxes overlap on shared faces with different
+    values there, so the order in which sources win is exercised too."""
+    rng = np.random.default_rng(8)
+    coarse = [((i, j, k), (i + 8, j + 8, k + 8)) for k in (0, 8) for j in (0, 8, 16)
+              for i in (0, 8, 16, 24)]  # shared faces
+    patches = fine_patches(3, ("interpolate", 3, 0), n=12)
+    ex = CoarsePatchExchange(coarse, [0] * len(coarse), patches, [0] * len(patches), 0)
+    shape = lambda b: tuple(b[1][d] - b[0][d] + 1 for d in (2, 1, 0))  # noqa: E731
+    cdat = {ci: rng.uniform(-1, 1, (2,) + shape(b)) for ci, b in enumerate(coarse)}
+    host_c = {ci: torch.from_numpy(a) for ci, a in cdat.items()}
+    host_p = {pi: torch.full((2,) + shape(b), np.nan, dtype=torch.float64)
+              for pi, b in enumerate(patches)}
+    dev_c = {ci: t.to(dev) for ci, t in host_c.items()}
+    dev_p = {pi: t.to(dev) for pi, t in host_p.items()}
+    ex.run(host_c, host_p)
+    ex.run(dev_c, dev_p)
+    assert ex._plan is not None
+    for pi in host_p:
+        a, b = host_p[pi].numpy(), dev_p[pi].cpu().numpy()
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), f"patch {pi}"
