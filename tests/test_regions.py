@@ -128,3 +128,24 @@ def test_copy_plan_rejects():
     assert plan_status("fb", good, None, 0, (1, 1, 1), None, (0, 0, 0))[0] == cb.CX_EINVAL
     assert plan_status("fb", good, None, 1, (-1, 1, 1), None, (0, 0, 0))[0] == cb.CX_EINVAL
     assert plan_status("fb", good, None, 1, (1, 1, 1), None, (-4, 0, 0))[0] == cb.CX_EINVAL
+
+
+def test_restrict_plan_rejects_without_device():
+    """cx_restrict_plan_create checks every box as cx_restrict_box does,
+    before it touches a device: a region outside the coarse box is
+    CX_EINVAL, an index type outside 0..7 CX_EUNSUPPORTED, and the failing
+    box is named."""
+    import carpetx_b200 as cb
+    L = cb.lib()
+
+    def box(it, rhi):
+        return cb.CxRestrictBox(it, 1, 0x10000, cb._i3((0, 0, 0)), cb._i3((7, 7, 7)), 0x20000,
+                                cb._i3((0, 0, 0)), cb._i3((3, 3, 3)), cb._i3((0, 0, 0)),
+                                cb._i3(rhi))
+
+    h = ctypes.c_void_p()
+    arr = (cb.CxRestrictBox * 2)(box(7, (3, 3, 3)), box(7, (4, 3, 3)))
+    assert L.cx_restrict_plan_create(arr, 2, ctypes.byref(h)) == cb.CX_EINVAL
+    assert "box 1" in L.cx_last_error().decode()
+    arr = (cb.CxRestrictBox * 1)(box(8, (3, 3, 3)))
+    assert L.cx_restrict_plan_create(arr, 1, ctypes.byref(h)) == cb.CX_EUNSUPPORTED
