@@ -52,3 +52,13 @@ def test_gpu_sync_chain_matches_oracle(cx, dev):
     got = sc.gpu_chain(cx, 11, dev)
     for i, (g, w) in enumerate(zip(got, want)):
         assert_bitwise(g, w, f"fine FAB {i}")
+
+
+@pytest.mark.gpu
+def test_gpu_sync_chain_graph_replay(cx, dev):
+    """The six plan executions of a sync captured into one CUDA graph and
+    replayed twice give the host chain's result bit for bit."""
+    want = sc.oracle_chain(cx, 12)
+    got = sc.gpu_chain(cx, 12, dev, graph=True)
+    for i, (g, w) in enumerate(zip(got, want)):
+        assert_bitwise(g, w, f"fine FAB {i}")
