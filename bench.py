@@ -555,6 +555,31 @@ def cpu_threads():
     return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
 
 
+def cpu_model():
+    """The host CPU's model name (as lscpu reports it), from /proc/cpuinfo."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_timed_passes(lib, kind, boxes, crse, fine, min_s=5.0, min_passes=5, max_passes=200):
+    """Passes of the reference CPU path over the sample after two warm-up
+    passes, until min_s seconds and min_passes passes are reached; returns
+    (total seconds, passes)."""
+    for _ in range(2):
+        cpu_run(lib, kind, boxes, crse, fine)
+    t, n = 0.0, 0
+    while n < max_passes and (t < min_s or n < min_passes):
+        t += cpu_run(lib, kind, boxes, crse, fine)
+        n += 1
+    return t, n
+
+
 def run_reference(args, rank):
     """--impl reference: the reference's own CPU implementation of the path on
     the host cores, same workload, one component of every box per step."""
@@ -576,7 +601,7 @@ def run_reference(args, rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference", "config": cfg,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
-                             "sample": sample},
+                             "cpu_model": cpu_model(), "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -822,13 +847,13 @@ def main():
         lib, kind = cpu_lib()
         cboxes = boxes
         c_crse, c_fine = cpu_sample(cboxes, args.seed)
-        cpu_run(lib, kind, cboxes, c_crse, c_fine)  # warm-up
-        t = cpu_run(lib, kind, cboxes, c_crse, c_fine)
+        t, npass = cpu_timed_passes(lib, kind, cboxes, c_crse, c_fine)
         pts = sum(npts(b[5], b[6]) for b in cboxes)
-        line["cpu_baseline"] = {"value": pts / t, "unit": UNIT, "cores": cpu_threads(),
-                                "kind": kind,
+        line["cpu_baseline"] = {"value": pts * npass / t, "unit": UNIT, "cores": cpu_threads(),
+                                "cpu_model": cpu_model(), "kind": kind,
                                 "sample": f"component 0 of all {len(cboxes)} boxes "
-                                          f"({pts} fine points), one pass after one warm-up"}
+                                          f"({pts} fine points) per pass, {npass} passes "
+                                          f"({t:.1f} s) after two warm-up passes"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     plan.close()

@@ -1,6 +1,8 @@
 // Host side of the adjoint of the separable linear prolongations: kernel
 // lookup per stencil pair and centring, tiling, launches.  The kernel is in
 // adjoint_kernel.cuh; its instantiations are spread over adjoint_part*.cu.
+#include <atomic>
+
 #include "adjoint_kernel.cuh"
 
 namespace cxb {
@@ -40,24 +42,31 @@ int adj_upt(int pair) {
   return 2;
 }
 
-bool g_adj_attr[kAdjGroups] = {};
-int g_adj_grid[kAdjGroups] = {};
+// Per device (cache_device()): dynamic shared memory allowed and persistent
+// grid per group (0: not yet set up on that device).
+std::atomic<int> g_adj_grid[kMaxDevices][kAdjGroups];
 
 // Kernel of a group, its dynamic shared memory allowed and its persistent
-// grid (SMs x resident CTAs) recorded on first use.
-AdjFn adj_ready(int group, size_t *smem) {
+// grid (SMs x resident CTAs) recorded on first use on the current device.
+AdjFn adj_ready(int group, size_t *smem, int *grid) {
   AdjFn k = adj_kernel(group, smem);
-  if (k && !g_adj_attr[group]) {
-    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem) !=
-        cudaSuccess)
-      return nullptr;
-    int per_sm = 0, dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, *smem);
-    g_adj_grid[group] = sms * (per_sm > 0 ? per_sm : 1);
-    g_adj_attr[group] = true;
+  if (!k)
+    return nullptr;
+  const int dev = cache_device();
+  if (dev >= 0 && g_adj_grid[dev][group].load()) {
+    *grid = g_adj_grid[dev][group].load();
+    return k;
   }
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem) !=
+      cudaSuccess)
+    return nullptr;
+  int per_sm = 0, d = 0, sms = 0;
+  cudaGetDevice(&d);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, *smem);
+  *grid = sms * (per_sm > 0 ? per_sm : 1);
+  if (dev >= 0)
+    g_adj_grid[dev][group].store(*grid);
   return k;
 }
 
@@ -114,7 +123,8 @@ void adjoint_tiling(BoxDesc &b, int min_items) {
 
 int adjoint_level_grid(int group) {
   size_t smem = 0;
-  return adj_ready(group, &smem) ? g_adj_grid[group] : 0;
+  int grid = 0;
+  return adj_ready(group, &smem, &grid) ? grid : 0;
 }
 
 cudaError_t launch_prolong_adjoint_box(const BoxDesc &b0, int per_group, double *crse_bar,
@@ -124,18 +134,18 @@ cudaError_t launch_prolong_adjoint_box(const BoxDesc &b0, int per_group, double 
     return cudaSuccess;
   const int group = adjoint_group_of(b0);
   size_t smem = 0;
-  AdjFn k = adj_ready(group, &smem);
+  int grid = 0;
+  AdjFn k = adj_ready(group, &smem, &grid);
   if (!k)
     return cudaErrorInvalidValue;
   BoxDesc b = b0;
   b.cbar = crse_bar;
-  adjoint_tiling(b, g_adj_grid[group]);
+  adjoint_tiling(b, grid);
   const int64_t n64 = (int64_t)b.ant[0] * b.ant[1] * b.ant[2] * b.ncomp;
   if (n64 > INT32_MAX)
     return cudaErrorInvalidValue;
   const int n = (int)n64;
-  k<<<n < g_adj_grid[group] ? n : g_adj_grid[group], NT, smem, s>>>(b, nullptr, nullptr, n,
-                                                                     nullptr);
+  k<<<n < grid ? n : grid, NT, smem, s>>>(b, nullptr, nullptr, n, nullptr);
   return cudaGetLastError();
 }
 
@@ -145,7 +155,8 @@ cudaError_t launch_adjoint_level(int group, const BoxDesc *d_boxes, const TileRe
   if (nitems <= 0)
     return cudaSuccess;
   size_t smem = 0;
-  AdjFn k = adj_ready(group, &smem);
+  int unused_grid = 0;
+  AdjFn k = adj_ready(group, &smem, &unused_grid);
   if (!k)
     return cudaErrorInvalidValue;
   BoxDesc unused{};

@@ -7,6 +7,21 @@
 
 namespace cxb {
 
+// Per-device caches of kernel attributes and persistent grid sizes:
+// cudaFuncSetAttribute and the SM count apply per device, so a process
+// driving several GPUs keeps one entry per device.  Devices with an index
+// at or above kMaxDevices are served uncached.
+constexpr int kMaxDevices = 64;
+// The current device if it can be cached, else -1.
+inline int cache_device() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return d >= 0 && d < kMaxDevices ? d : -1;
+}
+
 // Streaming kernel: threads per CTA (kStrThreadsSmall for the items of
 // boxes with at most kStrSmallUnits column units per x chunk), column units
 // per thread, fine y per unit (kStrFineYPerUnit / 2 coarse y centres); at

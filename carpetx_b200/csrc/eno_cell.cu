@@ -19,6 +19,7 @@
 // children with interp1d<CC,ENO,2> (impl.hxx:806-841) in call_stencil_3d's
 // order (x lines, then y, then z), sharing the x and y results between the
 // children: 38 1-D evaluations per cell instead of 8 x 13.
+#include <atomic>
 #include "cx_internal.h"
 #include "cx_stencils.cuh"
 
@@ -336,8 +337,9 @@ __global__ void __launch_bounds__(ENT, 2)
   asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
-bool g_eno_attr = false;
-int g_eno_grid = 0;
+// Per device (cache_device()): persistent grid, 0 until the kernel's dynamic
+// shared memory has been allowed on that device.
+std::atomic<int> g_eno_grid[kMaxDevices];
 
 } // namespace
 
@@ -362,20 +364,23 @@ cudaError_t launch_eno_cell_box(const BoxDesc &b, int per_group, signed char *sh
   const int64_t n = (int64_t)t.nt[0] * t.nt[1] * t.nt[2] * t.nblk;
   if (n > INT32_MAX)
     return cudaErrorInvalidValue;
-  if (!g_eno_attr) {
+  const int dev = cache_device();
+  int grid = dev >= 0 ? g_eno_grid[dev].load() : 0;
+  if (!grid) {
     cudaError_t e = cudaFuncSetAttribute(eno_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)sizeof(EnoShared));
     if (e != cudaSuccess)
       return e;
-    int per_sm = 0, dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int per_sm = 0, d = 0, sms = 0;
+    cudaGetDevice(&d);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eno_cell_kernel, ENT, sizeof(EnoShared));
-    g_eno_grid = sms * (per_sm > 0 ? per_sm : 1);
-    g_eno_attr = true;
+    grid = sms * (per_sm > 0 ? per_sm : 1);
+    if (dev >= 0)
+      g_eno_grid[dev].store(grid);
   }
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(n < g_eno_grid ? (unsigned)n : (unsigned)g_eno_grid);
+  cfg.gridDim = dim3(n < grid ? (unsigned)n : (unsigned)grid);
   cfg.blockDim = dim3(ENT);
   cfg.dynamicSmemBytes = sizeof(EnoShared);
   cfg.stream = s;

@@ -1,12 +1,13 @@
 // Allocation-free level transfer: cx_level_execute_noalloc.
 //
-// For callers that cannot allocate device memory, for example code running
-// inside a CUDA-graph capture that must stay replayable without a pool, a
-// host framework whose allocator owns all device memory, or callers that have
-// already handed all device memory to their own allocator.  The level plan
-// (cx_level_plan_create) allocates its device work list with cudaMalloc; this
-// entry point instead keeps the work list in one fixed device array, declared
-// below, that every GPU loading the library holds until the process exits.
+// For callers that cannot allocate device memory while they transfer a
+// level: a host framework whose own allocator owns all device memory, or
+// code that has already handed every byte of the GPU to such an allocator,
+// so that a cudaMalloc would fail or would take memory the framework counts
+// on.  The level plan (cx_level_plan_create) allocates its device work list
+// with cudaMalloc; this entry point instead keeps the work list in one fixed
+// device array, declared below, that every GPU loading the library holds
+// until the process exits.
 //
 // The work list is built on the host in a static staging buffer under a
 // mutex and copied into the device array on the caller's stream; then the
@@ -48,7 +49,8 @@ constexpr int kMaxDevices = 64;
 WorkList *g_dev_scratch[kMaxDevices] = {}; // device address of g_scratch per device
 
 // Device address of g_scratch for the current device, looked up once per
-// device (with that device current) and cached.
+// device (with that device current) and cached; called with g_lock held, so
+// two threads making their first call at once do not race on the cache.
 int scratch_address(WorkList **out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
@@ -84,11 +86,11 @@ extern "C" int cx_level_execute_noalloc(const cx_box_t *boxes, int nboxes, int p
   if (nboxes > kMaxBoxes)
     return record_failure(CX_EINVAL, "too many boxes for the allocation-free level transfer "
                                      "(at most CX_NOALLOC_MAX_BOXES)");
+  cudaStream_t s = (cudaStream_t)stream;
+  std::lock_guard<std::mutex> guard(g_lock);
   WorkList *dev = nullptr;
   if (int e = scratch_address(&dev))
     return e;
-  cudaStream_t s = (cudaStream_t)stream;
-  std::lock_guard<std::mutex> guard(g_lock);
   // boxes, validated as cx_prolong_box does
   int nb = 0;
   bool point[kMaxBoxes];

@@ -1,4 +1,6 @@
 // Host side of the streaming kernel: pair lookup, tiling, launches.
+#include <atomic>
+
 #include "stream_kernel.cuh"
 #include "stream_pairs.h"
 
@@ -14,7 +16,11 @@ KernelFn kernel_part6(int group, bool small_cta);
 KernelFn kernel_part7(int group, bool small_cta);
 
 namespace {
-bool g_attr_set[kStrGroups] = {};
+// Per device (cache_device()): dynamic shared memory allowed per group
+// (the attribute applies per device), SM count, persistent grid per group.
+std::atomic<bool> g_attr_set[kMaxDevices][kStrGroups];
+std::atomic<int> g_sms[kMaxDevices];
+std::atomic<int> g_grid[kMaxDevices][kStrGroups];
 
 // Threads and dynamic shared memory of a level group's CTA size.
 int threads_of(int group) { return group >= kStrKinds ? small::NTS : big::NTS; }
@@ -23,8 +29,8 @@ size_t smem_of(int group) {
 }
 
 // Kernel of a level group (instantiation + kStrKinds for the 128-thread
-// variant); the first lookup allows its dynamic shared memory, which may
-// exceed the 48 KB default.
+// variant); the first lookup on a device allows its dynamic shared memory,
+// which may exceed the 48 KB default.
 KernelFn kernel_for(int group) {
   if (group < 0 || group >= kStrGroups)
     return nullptr;
@@ -33,23 +39,25 @@ KernelFn kernel_for(int group) {
       kernel_part4, kernel_part5, kernel_part6, kernel_part7};
   const int kind = group % kStrKinds;
   KernelFn k = parts[kind % kStreamParts](kind, group >= kStrKinds);
-  if (k && !g_attr_set[group]) {
+  const int dev = cache_device();
+  if (k && (dev < 0 || !g_attr_set[dev][group].load())) {
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_of(group));
-    g_attr_set[group] = true;
+    if (dev >= 0)
+      g_attr_set[dev][group].store(true);
   }
   return k;
 }
 
-int g_sms = 0;
-int g_grid[kStrGroups] = {};
-
 int sms() {
-  if (!g_sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
-  }
-  return g_sms;
+  const int dev = cache_device();
+  if (dev >= 0 && g_sms[dev].load())
+    return g_sms[dev].load();
+  int d = 0, n = 0;
+  cudaGetDevice(&d);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, d);
+  if (dev >= 0)
+    g_sms[dev].store(n);
+  return n;
 }
 } // namespace
 } // namespace stream
@@ -131,12 +139,15 @@ int stream_level_grid(int group) {
   KernelFn k = kernel_for(group);
   if (!k)
     return 0;
-  if (!g_grid[group]) {
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads_of(group), smem_of(group));
-    g_grid[group] = sms() * (per_sm > 0 ? per_sm : 1);
-  }
-  return g_grid[group];
+  const int dev = cache_device();
+  if (dev >= 0 && g_grid[dev][group].load())
+    return g_grid[dev][group].load();
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads_of(group), smem_of(group));
+  const int grid = sms() * (per_sm > 0 ? per_sm : 1);
+  if (dev >= 0)
+    g_grid[dev][group].store(grid);
+  return grid;
 }
 
 cudaError_t launch_stream_box(const BoxDesc &b, cudaStream_t s) {

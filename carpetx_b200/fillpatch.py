@@ -138,7 +138,11 @@ class CoarsePatchExchange:
         if not all(getattr(t, "is_cuda", False) and str(t.dtype) == "torch.float64"
                    for t in ts):
             return None
-        key = tuple(t.data_ptr() for t in ts)
+        # the caching allocator can hand a freed address to a tensor of
+        # another shape, so the key holds each tensor's extents and strides
+        # (and with them ncomp) beside its address and device
+        key = tuple((t.data_ptr(), t.device.index, tuple(t.shape), tuple(t.stride()))
+                    for t in ts)
         if key != self._plan_key:
             from carpetx_b200 import CopyPlan
             ncomp = int(ts[0].shape[0])

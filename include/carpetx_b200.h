@@ -171,7 +171,9 @@ int cx_level_plan_create_adjoint(const cx_box_t *boxes, int nboxes,
 #define CX_NOALLOC_MAX_ITEMS 131072
 
 /* The level transfer of cx_level_plan_create + cx_level_plan_execute, for
- * callers that cannot allocate device memory: there is no plan object; the
+ * callers that cannot allocate device memory, such as a host framework whose
+ * own allocator owns all device memory (a cudaMalloc of ours would fail, or
+ * would take memory that allocator counts on): there is no plan object; the
  * work list lives in one fixed device array of the library (about 1.7 MB per
  * GPU, held until the process exits) and is rebuilt and copied onto `stream`
  * at every call.  Allocates nothing: no cudaMalloc, no cudaFree, no

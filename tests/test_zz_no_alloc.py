@@ -1,9 +1,8 @@
 """The allocation-free level transfer, cx_level_execute_noalloc.
 
 Some callers cannot allocate device memory while they transfer a level:
-- code that runs inside a CUDA-graph capture and must stay replayable without
-  a memory pool;
-- a host framework whose own allocator owns all device memory;
+- a host framework whose own allocator owns all device memory, where a
+  cudaMalloc of ours would fail or take memory that allocator counts on;
 - callers that have already handed every byte of the GPU to their allocator.
 
 cx_level_plan_create allocates the device work list with cudaMalloc; this
