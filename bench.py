@@ -273,28 +273,30 @@ def restrict_leg(args, cb, torch, dev, max_over_ranks, barrier, peak):
 
 def limited_leg(args, cb, torch, dev, max_over_ranks, barrier):
     """Limited operators of the shock configuration: ENO order 3 and minmod,
-    all directions cell centred, 64 boxes of 64^3 coarse cells (3 ghosts),
-    5 variables, a level plan each (the pointwise kernel).  The values are a
-    planar shock with jumps of 10x and Fourier modes on top, so the ENO shift
-    search and the minmod branches see both smooth and discontinuous data."""
-    nc, nb = 5, 64
-    flo, fhi = (0, 0, 0), (127, 127, 127)
-    out = {"workload": f"{nb} boxes, 64^3 coarse cells -> 128^3 fine, {nc} vars, CCC; level "
-                       "plans", "fine_points": nb * nc * npts(flo, fhi)}
-    gen = torch.Generator(device=dev)
-    gen.manual_seed(args.seed + 4)
+    all directions cell centred, 64 boxes of 64^3 coarse cells (3 ghosts)
+    tiling a 256^3-cell cube, 5 variables (rho, momenta, E) of the seeded
+    shock state of carpetx_b200.workloads.shock_state: a planar shock with a
+    random normal, 10x density and pressure jumps, Gaussian blobs and 1e-6
+    noise.  A level plan each; the data is generated on the host once."""
+    from carpetx_b200.workloads import shock_fab, shock_level_boxes, shock_state
+    nc = 5
+    state = shock_state(args.seed + 4, 256)
+    sboxes = shock_level_boxes()
+    nb = len(sboxes)
+    flo0, fhi0 = sboxes[0][3], sboxes[0][4]
+    out = {"workload": f"{nb} boxes, 64^3 coarse cells -> 128^3 fine, {nc} vars (rho, momenta, "
+                       "E) of a planar shock (random normal, 10x rho and p jumps) with Gaussian "
+                       "blobs and 1e-6 noise, CCC; level plans",
+           "fine_points": nb * nc * npts(flo0, fhi0)}
+    crse = [torch.from_numpy(shock_fab(state, clo, chi, bid)).to(dev)
+            for bid, clo, chi, flo, fhi in sboxes]
+    fine = [torch.empty((nc,) + box_shape(flo, fhi), dtype=torch.float64, device=dev)
+            for bid, clo, chi, flo, fhi in sboxes]
     for typ, order in (("eno", 3), ("minmod", 1)):
         op = cb.Op(typ, order, 7)
-        clo, chi = op.coarse_box(flo, fhi)
-        shape = (nc,) + box_shape(clo, chi)
-        z = torch.arange(shape[1], dtype=torch.float64, device=dev).view(1, -1, 1, 1)
-        boxes = []
-        for i in range(nb):
-            u = torch.randn(shape, dtype=torch.float64, device=dev, generator=gen) * 1e-2
-            u += torch.where(z > shape[1] * (0.3 + 0.4 * i / nb), 10.0, 1.0)
-            fine = torch.empty((nc,) + box_shape(flo, fhi), dtype=torch.float64, device=dev)
-            boxes.append(dict(op=op, ncomp=nc, crse=u, crse_lo=clo, crse_hi=chi, fine=fine,
-                              fine_lo=flo, fine_hi=fhi, reg_lo=flo, reg_hi=fhi))
+        boxes = [dict(op=op, ncomp=nc, crse=c, crse_lo=clo, crse_hi=chi, fine=f, fine_lo=flo,
+                      fine_hi=fhi, reg_lo=flo, reg_hi=fhi)
+                 for (bid, clo, chi, flo, fhi), c, f in zip(sboxes, crse, fine)]
         plan = cb.LevelPlan(boxes)
         for _ in range(2):
             plan.execute()
@@ -308,6 +310,7 @@ def limited_leg(args, cb, torch, dev, max_over_ranks, barrier):
         ms = max_over_ranks(e0.elapsed_time(e1)) / args.limited_steps
         out[f"{typ}_ms"] = ms
         out[f"{typ}_pts_per_s"] = out["fine_points"] / (ms / 1e3)
+        out[f"{typ}_launches"] = plan.stats()["launches"]
         plan.close()
         del boxes
     return out

@@ -110,3 +110,72 @@ def tiled_level_fabs(domain_n, box_n, indextype, nghost):
 # kind of condition: reflection (x lower), Dirichlet (x upper), linear
 # extrapolation (y lower, z upper), Robin (y upper), Neumann (z lower).
 BC_LEVEL_FACES = [[(3, 0), (0, 3), (0, 4)], [(0, 2), (0, 5), (0, 3)]]
+
+
+def shock_level_boxes(nb_dir=4, n=64, ghosts=3):
+    """The boxes of the shock level: nb_dir^3 boxes of n^3 coarse cells
+    tiling a cube of (nb_dir n)^3 cells, cell centred.  Per box (index,
+    crse_lo, crse_hi, fine_lo, fine_hi): the coarse FAB holds `ghosts` ghost
+    cells per side, the fine region is the whole refined box."""
+    out = []
+    for k in range(nb_dir):
+        for j in range(nb_dir):
+            for i in range(nb_dir):
+                t = (i, j, k)
+                clo = tuple(t[d] * n - ghosts for d in range(3))
+                chi = tuple((t[d] + 1) * n - 1 + ghosts for d in range(3))
+                flo = tuple(2 * t[d] * n for d in range(3))
+                fhi = tuple(2 * (t[d] + 1) * n - 1 for d in range(3))
+                out.append((len(out), clo, chi, flo, fhi))
+    return out
+
+
+def shock_state(seed, ncells):
+    """Parameters of the seeded hydro-like state on a cube of `ncells` cells
+    per direction (unit cube, cell centres at (i + 1/2) / ncells): a planar
+    shock with a random unit normal through a random point near the centre,
+    density and pressure 10x larger on the upstream side; a random velocity
+    per side; eight Gaussian blobs added to density and pressure; U[-1e-6,
+    1e-6] noise on every variable."""
+    rng = np.random.default_rng(seed)
+    nrm = rng.standard_normal(3)
+    nrm /= np.linalg.norm(nrm)
+    return {
+        "ncells": int(ncells),
+        "normal": nrm,
+        "offset": float(nrm @ np.full(3, 0.5) + rng.uniform(-0.15, 0.15)),
+        "rho": (1.0, 0.1), "p": (1.0, 0.1),  # upstream, downstream: jumps of 10x
+        "vel": rng.uniform(-1, 1, (2, 3)),
+        "blob_c": rng.uniform(0, 1, (8, 3)),
+        "blob_w": rng.uniform(0.02, 0.08, 8),
+        "blob_a": rng.uniform(0.05, 0.3, 8),
+        "gamma": 1.4,
+        "noise_seed": int(rng.integers(2**31)),
+    }
+
+
+def shock_fab(state, lo, hi, box_id=0):
+    """The 5 conserved variables (rho, rho vx, rho vy, rho vz, E) of the
+    shock state on the inclusive cell box [lo, hi], shape (5, nz, ny, nx),
+    FP64 on the host.  Ghost cells get the same smooth-plus-jump function,
+    so neighbouring FABs agree where they overlap; the noise is seeded per
+    box."""
+    shape = box_shape(lo, hi)
+    h = 1.0 / state["ncells"]
+    ax = [(np.arange(lo[d], hi[d] + 1, dtype=float) + 0.5) * h for d in range(3)]
+    z, y, x = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
+    n = state["normal"]
+    up = (n[0] * x + n[1] * y + n[2] * z) < state["offset"]
+    rho = np.where(up, state["rho"][0], state["rho"][1])
+    p = np.where(up, state["p"][0], state["p"][1])
+    blob = np.zeros(shape)
+    for c, w, a in zip(state["blob_c"], state["blob_w"], state["blob_a"]):
+        blob += a * np.exp(-((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2) / (2 * w * w))
+    rho = rho * (1.0 + blob)
+    p = p * (1.0 + blob)
+    vel = [np.where(up, state["vel"][0][d], state["vel"][1][d]) for d in range(3)]
+    e = p / (state["gamma"] - 1) + 0.5 * rho * (vel[0] ** 2 + vel[1] ** 2 + vel[2] ** 2)
+    out = np.stack([rho, rho * vel[0], rho * vel[1], rho * vel[2], e])
+    rng = np.random.default_rng(state["noise_seed"] + 7919 * int(box_id))
+    out += rng.uniform(-1e-6, 1e-6, out.shape)
+    return out
