@@ -163,6 +163,7 @@ def lib():
         L.cx_restrict_plan_stats.argtypes = [_VP, ctypes.POINTER(ctypes.c_int64),
                                              ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(_I)]
         L.cx_restrict_plan_destroy.argtypes = [_VP]
+        L.cx_debug_set_wait_limit.argtypes = [ctypes.c_longlong]
         _lib = L
     return _lib
 

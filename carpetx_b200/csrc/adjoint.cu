@@ -72,6 +72,18 @@ AdjFn adj_ready(int group, size_t *smem, int *grid) {
 
 } // namespace
 
+int adjoint_set_wait_limit(long long cycles) {
+  static int (*const parts[kStreamParts])(long long) = {
+      adj_set_wait_limit_part0, adj_set_wait_limit_part1, adj_set_wait_limit_part2,
+      adj_set_wait_limit_part3, adj_set_wait_limit_part4, adj_set_wait_limit_part5,
+      adj_set_wait_limit_part6, adj_set_wait_limit_part7};
+  const long long v = cycles >= 0 ? cycles : kWaitCycles;
+  for (auto f : parts)
+    if (f(v) != 0)
+      return -1;
+  return 0;
+}
+
 int adjoint_take_timeout() {
   static int (*const parts[kStreamParts])() = {adj_timeout_part0, adj_timeout_part1,
                                                adj_timeout_part2, adj_timeout_part3,

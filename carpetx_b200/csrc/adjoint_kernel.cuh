@@ -193,8 +193,13 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // Set when a bounded wait gave up (read and cleared by cx_check_device);
 // every translation unit that instantiates the kernels has its own copy.
+// g_adj_wait_limit: cycles a wait for a plane's copies polls before giving
+// up (kWaitCycles, about a second, unless cx_debug_set_wait_limit lowered it
+// to force the give-up path in a test); the copies still in flight when a CTA
+// gives up are always waited for with the default bound.
 namespace {
 __device__ int g_adj_timeout = 0;
+__device__ long long g_adj_wait_limit = kWaitCycles;
 }
 
 // y^T task: YB coarse y of one footprint column from a register window
@@ -418,16 +423,25 @@ __device__ __forceinline__ bool adj_item(double *fbuf, double *gbuf, uint64_t *m
     cp_async_commit();
     cp_async_wait_dpf();
     const uint32_t par = (phase >> slot) & 1u;
-    if (tid == 0 && !mbar_wait_bounded(mbar + slot, par)) {
+    if (tid == 0 && !mbar_wait_bounded(mbar + slot, par, g_adj_wait_limit)) {
       *s_fail = 1;
       g_adj_timeout = 1;
     }
     __syncthreads();
     if (*s_fail) {
-      // stop: let the copies issued for the next plane land first (bounded)
-      if (tid == 0 && more) {
-        mbar_arrive(mbar + ls);
-        mbar_wait_bounded(mbar + ls, (phase >> ls) & 1u);
+      // stop, once every copy still in flight into this CTA's buffers has
+      // landed (each wait bounded by the default): planes fz .. fz + DPF - 1
+      // were issued and arrived on earlier, plane fz + DPF was issued just
+      // now and is arrived on here; then the 8-byte copies
+      if (tid == 0) {
+        if (more)
+          mbar_arrive(mbar + ls);
+        for (int d = 0; d <= DPF && fz + d <= fb; ++d) {
+          int k = slot + d;
+          if (k >= NBUF)
+            k -= NBUF;
+          mbar_wait_bounded(mbar + k, (phase >> k) & 1u, kWaitCycles);
+        }
       }
       cp_async_wait_all();
       __syncthreads();
@@ -567,6 +581,15 @@ AdjFn adj_kernel_part4(int pair, size_t *smem);
 AdjFn adj_kernel_part5(int pair, size_t *smem);
 AdjFn adj_kernel_part6(int pair, size_t *smem);
 AdjFn adj_kernel_part7(int pair, size_t *smem);
+// Sets that file's wait limit (cycles); 0 on success, -1 on a CUDA error.
+int adj_set_wait_limit_part0(long long cycles);
+int adj_set_wait_limit_part1(long long cycles);
+int adj_set_wait_limit_part2(long long cycles);
+int adj_set_wait_limit_part3(long long cycles);
+int adj_set_wait_limit_part4(long long cycles);
+int adj_set_wait_limit_part5(long long cycles);
+int adj_set_wait_limit_part6(long long cycles);
+int adj_set_wait_limit_part7(long long cycles);
 int adj_timeout_part0();
 int adj_timeout_part1();
 int adj_timeout_part2();

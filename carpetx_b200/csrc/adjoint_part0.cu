@@ -1,6 +1,7 @@
 // Adjoint-kernel instantiations of centring 0 ((cx << 2) | (cy << 1) | cz),
 // one per linear stencil pair of stream_pairs.h; split only to compile in
-// parallel.  This file's copy of the timeout flag is read here.
+// parallel.  This file's copies of the timeout flag and the wait limit are
+// read and set here.
 #include "adjoint_kernel.cuh"
 
 namespace cxb {
@@ -17,6 +18,10 @@ AdjFn adj_kernel_part0(int pair, size_t *smem) {
     break;
   }
   return nullptr;
+}
+
+int adj_set_wait_limit_part0(long long cycles) {
+  return cudaMemcpyToSymbol(g_adj_wait_limit, &cycles, sizeof cycles) == cudaSuccess ? 0 : -1;
 }
 
 int adj_timeout_part0() {

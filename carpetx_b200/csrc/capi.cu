@@ -584,6 +584,16 @@ int cx_check_device(void) {
   return CX_OK;
 }
 
+int cx_debug_set_wait_limit(long long cycles) {
+  if (int e = check_device())
+    return e;
+  if (adjoint_set_wait_limit(cycles) != 0) {
+    cudaGetLastError();
+    return fail(CX_ECUDA, "setting the device wait limit failed");
+  }
+  return CX_OK;
+}
+
 int cx_level_plan_stats(cx_level_plan_t p, int64_t *ntiles, int64_t *nfine, int64_t *bytes) {
   if (!p)
     return fail(CX_EINVAL, "null plan");

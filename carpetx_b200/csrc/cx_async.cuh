@@ -33,12 +33,19 @@ __device__ __forceinline__ bool mbar_try(uint64_t *m, uint32_t parity) {
                : "memory");
   return ok != 0;
 }
-// Waits for the phase of parity `parity` to complete, for about a second at
-// most (clock cycles); false if it gave up.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *m, uint32_t parity) {
+// Default bound of a wait, in SM clock cycles: about a second.
+constexpr long long kWaitCycles = 1ll << 31;
+// Waits for the phase of parity `parity` to complete, polling for at most
+// `limit` clock cycles (each poll may suspend the thread for a short
+// hardware-defined time); false if it gave up.  A limit of 0 gives up at
+// once without polling: tests use it to force the give-up path.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *m, uint32_t parity,
+                                                  long long limit = kWaitCycles) {
+  if (limit <= 0)
+    return false;
   const long long t0 = clock64();
   while (!mbar_try(m, parity))
-    if (clock64() - t0 > (1ll << 31))
+    if (clock64() - t0 > limit)
       return false;
   return true;
 }

@@ -54,6 +54,16 @@ enum {
  * error, CX_OK otherwise.  Kernels never wait without a bound. */
 int cx_check_device(void);
 
+/* Sets, on the current device, how many SM clock cycles a kernel's bounded
+ * wait on its own asynchronous copies polls before it gives up; cycles < 0
+ * restores the default (2^31, about a second), cycles = 0 makes every such
+ * wait give up at once.  For tests of the give-up path: the kernels then
+ * return early, after letting every copy still in flight into their shared
+ * memory land (bounded by the default), and cx_check_device reports
+ * CX_ETIMEOUT.  Call it with the device idle.  No counterpart in the
+ * reference (its kernels never wait). */
+int cx_debug_set_wait_limit(long long cycles);
+
 /* Human-readable name of a status code. */
 const char *cx_status_string(int status);
 /* Text of the most recent failure on this thread ("" if none). */
