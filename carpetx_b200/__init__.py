@@ -82,6 +82,12 @@ class CxRestrictBox(ctypes.Structure):
                 ("reg_lo", _I3), ("reg_hi", _I3)]
 
 
+class CxRestrictGroup(ctypes.Structure):
+    """cx_restrict_group_t"""
+    _fields_ = [("indextype", _I), ("ncomp", _I), ("ntimelevels", _I), ("do_restrict", _I),
+                ("is_regrid_error", _I), ("nfabs", _I), ("fabs", ctypes.POINTER(CxRestrictBox))]
+
+
 class CxFab(ctypes.Structure):
     """cx_fab_t"""
     _fields_ = [("data", _VP), ("lo", _I3), ("hi", _I3), ("valid_lo", _I3), ("valid_hi", _I3)]
@@ -163,6 +169,8 @@ def lib():
         L.cx_restrict_plan_stats.argtypes = [_VP, ctypes.POINTER(ctypes.c_int64),
                                              ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(_I)]
         L.cx_restrict_plan_destroy.argtypes = [_VP]
+        L.cx_restrict_groups_plan_create.argtypes = [ctypes.POINTER(CxRestrictGroup), _I,
+                                                     ctypes.POINTER(_I), ctypes.POINTER(_VP)]
         L.cx_debug_set_wait_limit.argtypes = [ctypes.c_longlong]
         _lib = L
     return _lib
@@ -318,6 +326,20 @@ class BoundaryPlan:
             pass
 
 
+def _restrict_boxes(boxes, keep):
+    arr = (CxRestrictBox * max(1, len(boxes)))()
+    for i, b in enumerate(boxes):
+        n = int(b["ncomp"])
+        arr[i] = CxRestrictBox(int(b["indextype"]), n,
+                               _ptr(b["fine"], n, b["fine_lo"], b["fine_hi"], "fine").value,
+                               _i3(b["fine_lo"]), _i3(b["fine_hi"]),
+                               _ptr(b["crse"], n, b["crse_lo"], b["crse_hi"], "crse").value,
+                               _i3(b["crse_lo"]), _i3(b["crse_hi"]), _i3(b["reg_lo"]),
+                               _i3(b["reg_hi"]))
+        keep += [b["fine"], b["crse"]]
+    return arr
+
+
 class RestrictPlan:
     """cx_restrict_plan_*: the restriction of a whole level (every FAB pair,
     all components) in one launch per index type.  boxes: dicts with keys
@@ -326,20 +348,45 @@ class RestrictPlan:
 
     def __init__(self, boxes):
         boxes = list(boxes)
-        arr = (CxRestrictBox * max(1, len(boxes)))()
         self._keep = []
-        for i, b in enumerate(boxes):
-            n = int(b["ncomp"])
-            arr[i] = CxRestrictBox(int(b["indextype"]), n,
-                                   _ptr(b["fine"], n, b["fine_lo"], b["fine_hi"], "fine").value,
-                                   _i3(b["fine_lo"]), _i3(b["fine_hi"]),
-                                   _ptr(b["crse"], n, b["crse_lo"], b["crse_hi"], "crse").value,
-                                   _i3(b["crse_lo"]), _i3(b["crse_hi"]), _i3(b["reg_lo"]),
-                                   _i3(b["reg_hi"]))
-            self._keep += [b["fine"], b["crse"]]
+        arr = _restrict_boxes(boxes, self._keep)
         h = ctypes.c_void_p()
         _check(lib().cx_restrict_plan_create(arr, len(boxes), ctypes.byref(h)))
         self.handle = h
+        self.restricted = None
+
+    @classmethod
+    def for_groups(cls, groups):
+        """cx_restrict_groups_plan_create: Restrict() of one level
+        (CarpetX/src/schedule.cxx:2717-2837).  groups: dicts with keys
+        indextype, ncomp, ntimelevels, do_restrict, is_regrid_error and fabs
+        (per time level, newest first, a list of FAB-pair dicts as for the
+        constructor; every time level has the same number of pairs).  The
+        plan's `restricted` lists, per group, how many time levels it
+        restricts (0 for a skipped group)."""
+        groups = list(groups)
+        self = cls.__new__(cls)
+        self._keep = []
+        garr = (CxRestrictGroup * max(1, len(groups)))()
+        self._arrays = []
+        for g, gr in enumerate(groups):
+            tls = list(gr["fabs"])
+            nf = len(tls[0]) if tls else 0
+            if any(len(t) != nf for t in tls):
+                raise ValueError(f"group {g}: every time level needs the same FAB pairs")
+            flat = [b for t in tls for b in t]
+            arr = _restrict_boxes(flat, self._keep)
+            self._arrays.append(arr)
+            garr[g] = CxRestrictGroup(int(gr["indextype"]), int(gr["ncomp"]),
+                                      int(gr["ntimelevels"]), int(bool(gr["do_restrict"])),
+                                      int(bool(gr.get("is_regrid_error", False))), nf,
+                                      ctypes.cast(arr, ctypes.POINTER(CxRestrictBox)))
+        nres = (_I * max(1, len(groups)))()
+        h = ctypes.c_void_p()
+        _check(lib().cx_restrict_groups_plan_create(garr, len(groups), nres, ctypes.byref(h)))
+        self.handle = h
+        self.restricted = [int(nres[g]) for g in range(len(groups))]
+        return self
 
     def execute(self, stream=None):
         _check(lib().cx_restrict_plan_execute(self.handle, _stream(stream)))

@@ -576,7 +576,8 @@ int cx_check_device(void) {
     return e;
   if (int e = cuda_status(cudaDeviceSynchronize(), "device work"))
     return e;
-  const int t = adjoint_take_timeout();
+  const int ta = adjoint_take_timeout(), ts = stream_take_timeout();
+  const int t = ta < 0 || ts < 0 ? -1 : ta | ts;
   if (t < 0)
     return fail(CX_ECUDA, "reading the device wait flag failed");
   if (t > 0)
@@ -587,7 +588,7 @@ int cx_check_device(void) {
 int cx_debug_set_wait_limit(long long cycles) {
   if (int e = check_device())
     return e;
-  if (adjoint_set_wait_limit(cycles) != 0) {
+  if (adjoint_set_wait_limit(cycles) != 0 || stream_set_wait_limit(cycles) != 0) {
     cudaGetLastError();
     return fail(CX_ECUDA, "setting the device wait limit failed");
   }
@@ -747,6 +748,45 @@ int cx_restrict_plan_create(const cx_restrict_box_t *boxes, int nboxes, cx_restr
     }
   }
   *out = p;
+  return CX_OK;
+}
+
+int cx_restrict_groups_plan_create(const cx_restrict_group_t *groups, int ngroups,
+                                   int *restricted, cx_restrict_plan_t *out) {
+  if (!out || ngroups < 0 || (ngroups > 0 && (!groups || !restricted)))
+    return fail(CX_EINVAL, "invalid argument");
+  *out = nullptr;
+  std::vector<cx_restrict_box_t> sel;
+  for (int g = 0; g < ngroups; ++g) {
+    const cx_restrict_group_t &gr = groups[g];
+    restricted[g] = 0;
+    if (gr.indextype < 0 || gr.indextype > 7)
+      return fail(CX_EINVAL, "group %d: indextype %d out of range 0..7", g, gr.indextype);
+    if (gr.ntimelevels < 0 || gr.nfabs < 0 || gr.ncomp < 0 ||
+        (gr.ntimelevels > 0 && gr.nfabs > 0 && !gr.fabs))
+      return fail(CX_EINVAL, "group %d: invalid time levels, FABs or components", g);
+    // schedule.cxx:2746-2750: neither the regrid error nor a group with
+    // restriction disabled
+    if (gr.is_regrid_error || !gr.do_restrict)
+      continue;
+    // schedule.cxx:2755-2756: all time levels but the oldest, all of them
+    // when there is only one
+    const int ntl = gr.ntimelevels > 1 ? gr.ntimelevels - 1 : gr.ntimelevels;
+    for (int tl = 0; tl < ntl; ++tl)
+      for (int f = 0; f < gr.nfabs; ++f) {
+        const cx_restrict_box_t &b = gr.fabs[(int64_t)tl * gr.nfabs + f];
+        if (b.indextype != gr.indextype || b.ncomp != gr.ncomp)
+          return fail(CX_EINVAL, "group %d, time level %d, FAB %d: indextype or ncomp differs "
+                                 "from the group's", g, tl, f);
+        sel.push_back(b);
+      }
+    restricted[g] = ntl;
+  }
+  if (int e = cx_restrict_plan_create(sel.data(), (int)sel.size(), out)) {
+    for (int g = 0; g < ngroups; ++g)
+      restricted[g] = 0;
+    return e;
+  }
   return CX_OK;
 }
 

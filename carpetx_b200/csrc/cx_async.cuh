@@ -24,6 +24,14 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *m) {
                    smem_u32(m))
                : "memory");
 }
+// Arrives on m (one arrival) and raises its expected transaction bytes by
+// `bytes` in one step.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *m, uint32_t bytes) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(
+                   smem_u32(m)),
+               "r"(bytes)
+               : "memory");
+}
 __device__ __forceinline__ bool mbar_try(uint64_t *m, uint32_t parity) {
   uint32_t ok;
   asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"

@@ -150,6 +150,10 @@ int adjoint_level_grid(int group);
 // 1 if a bounded wait of the adjoint kernels gave up since the last call
 // (and clears the flag), 0 if not, -1 if the flag could not be read.
 int adjoint_take_timeout();
+// The same for the streaming kernels (their compute threads' waits for a
+// plane's copies).
+int stream_take_timeout();
+int stream_set_wait_limit(long long cycles);
 // Sets the adjoint kernels' wait limit on the current device (cycles <= 0:
 // the default, about a second); 0 on success, -1 on a CUDA error.
 int adjoint_set_wait_limit(long long cycles);

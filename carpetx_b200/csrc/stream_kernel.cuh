@@ -9,14 +9,18 @@
 // over a chunk of fine z; a unit is a fine x with FYT fine y (FYT / 2
 // coarse y centres, whose y windows overlap), units are numbered x fastest
 // over the box's x chunk (any width up to WFMAX), so every lane works on a
-// real fine point whatever the box shape.  The CTA streams the coarse z planes of the block's window
-// through a ring of shared-memory planes:
-//   load    plane c + DPF of the coarse window (asynchronous 8-byte copies,
-//           zero-filled outside the coarse points the operator reads);
+// real fine point whatever the box shape.  The CTA streams the coarse z
+// planes of the block's window through a ring of shared-memory planes:
+//   load    the producer warp copies plane c of the coarse window into a
+//           free slot of the ring, up to NRING planes ahead: one bulk copy
+//           (cp.async.bulk, no multicast) per window row, completing on the
+//           slot's mbarrier; only the coarse points the operator reads are
+//           copied;
 //   x pass  X[cy][fx] = interp_x(coarse row), XB fine x per task from a
-//           register window, into shared memory;
-//   y pass  each thread computes Y for the FYT fine y of each of its UPT
-//           units from a register window of X (consecutive lanes =
+//           register window, into shared memory; then the slot is released
+//           to the producer (an mbarrier arrival per compute warp);
+//   y pass  each compute thread computes Y for the FYT fine y of each of its
+//           UPT units from a register window of X (consecutive lanes =
 //           consecutive fine x);
 //   z pass  each thread keeps the Y values of the last L coarse planes in a
 //           register ring; once the ring holds the stencil of coarse centre
@@ -33,17 +37,29 @@
 // changes.
 //
 // The body (stream_body.cuh) is compiled for two CTA sizes: namespace big
-// (256 threads, 256 units per item) and namespace small (128 threads, 128
-// units) for boxes with at most 128 units per x chunk.  In a level, CTAs
+// (256 compute threads, 256 units per item) and namespace small (128 compute
+// threads, 128 units) for boxes with at most 128 units per x chunk; each has
+// the producer warp besides.  In a level, CTAs
 // take items from a per-launch counter, and each launch after a plan's
 // first is a programmatic dependent of the previous one.
 #pragma once
+#include "cx_async.cuh"
 #include "cx_internal.h"
 #include "cx_stencils.cuh"
 #include <type_traits>
 
 namespace cxb {
 namespace stream {
+
+// Set when a bounded wait gave up (read and cleared by cx_check_device);
+// g_str_wait_limit: cycles a compute thread's wait for a plane's copies polls
+// before giving up (kWaitCycles, about a second, unless
+// cx_debug_set_wait_limit lowered it to force the give-up path in a test).
+// Every translation unit that instantiates the kernels has its own copies.
+namespace {
+__device__ int g_str_timeout = 0;
+__device__ long long g_str_wait_limit = kWaitCycles;
+} // namespace
 
 namespace big {
 #define CXS_NTS kStrThreads

@@ -1,6 +1,8 @@
 // Host side of the streaming kernel: pair lookup, tiling, launches.
 #include <atomic>
 
+#include "cx_async.cuh"
+
 #include "stream_kernel.cuh"
 #include "stream_pairs.h"
 
@@ -14,6 +16,22 @@ KernelFn kernel_part4(int group, bool small_cta);
 KernelFn kernel_part5(int group, bool small_cta);
 KernelFn kernel_part6(int group, bool small_cta);
 KernelFn kernel_part7(int group, bool small_cta);
+int str_set_wait_limit_part0(long long);
+int str_set_wait_limit_part1(long long);
+int str_set_wait_limit_part2(long long);
+int str_set_wait_limit_part3(long long);
+int str_set_wait_limit_part4(long long);
+int str_set_wait_limit_part5(long long);
+int str_set_wait_limit_part6(long long);
+int str_set_wait_limit_part7(long long);
+int str_timeout_part0();
+int str_timeout_part1();
+int str_timeout_part2();
+int str_timeout_part3();
+int str_timeout_part4();
+int str_timeout_part5();
+int str_timeout_part6();
+int str_timeout_part7();
 
 namespace {
 // Per device (cache_device()): dynamic shared memory allowed per group
@@ -61,6 +79,35 @@ int sms() {
 }
 } // namespace
 } // namespace stream
+
+int stream_set_wait_limit(long long cycles) {
+  using namespace stream;
+  static int (*const parts[kStreamParts])(long long) = {
+      str_set_wait_limit_part0, str_set_wait_limit_part1, str_set_wait_limit_part2,
+      str_set_wait_limit_part3, str_set_wait_limit_part4, str_set_wait_limit_part5,
+      str_set_wait_limit_part6, str_set_wait_limit_part7};
+  const long long v = cycles >= 0 ? cycles : kWaitCycles;
+  for (auto f : parts)
+    if (f(v) != 0)
+      return -1;
+  return 0;
+}
+
+int stream_take_timeout() {
+  using namespace stream;
+  static int (*const parts[kStreamParts])() = {str_timeout_part0, str_timeout_part1,
+                                               str_timeout_part2, str_timeout_part3,
+                                               str_timeout_part4, str_timeout_part5,
+                                               str_timeout_part6, str_timeout_part7};
+  int any = 0;
+  for (auto f : parts) {
+    const int v = f();
+    if (v < 0)
+      return -1;
+    any |= v;
+  }
+  return any;
+}
 
 int stream_pair_of(int kx, int ky, int kz) {
   const int k[3] = {kx, ky, kz};

@@ -1,6 +1,7 @@
 // Streaming-kernel instantiations, part 3 of kStreamParts: the kernels whose
 // centring (cx << 2 | cy << 1 | cz) is 3, one per stencil pair of
-// stream_pairs.h and CTA size; split only to compile in parallel.
+// stream_pairs.h and CTA size; split only to compile in parallel.  This
+// file's copies of the timeout flag and the wait limit are read and set here.
 #include "stream_kernel.cuh"
 #include "stream_pairs.h"
 
@@ -18,6 +19,19 @@ KernelFn kernel_part3(int group, bool small_cta) {
     break;
   }
   return nullptr;
+}
+
+int str_set_wait_limit_part3(long long cycles) {
+  return cudaMemcpyToSymbol(g_str_wait_limit, &cycles, sizeof cycles) == cudaSuccess ? 0 : -1;
+}
+
+int str_timeout_part3() {
+  int v = 0, zero = 0;
+  if (cudaMemcpyFromSymbol(&v, g_str_timeout, sizeof v) != cudaSuccess)
+    return -1;
+  if (v)
+    cudaMemcpyToSymbol(g_str_timeout, &zero, sizeof zero);
+  return v;
 }
 
 } // namespace stream

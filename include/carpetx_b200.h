@@ -239,6 +239,31 @@ int cx_restrict_plan_stats(cx_restrict_plan_t plan, int64_t *ncoarse, int64_t *b
                            int *nlaunches);
 int cx_restrict_plan_destroy(cx_restrict_plan_t plan);
 
+/* Restrict() of one level (CarpetX/src/schedule.cxx:2717-2837): the groups
+ * to restrict from the next finer level, with the reference's selection.
+ * A group is skipped when it is the regrid error (CarpetXRegrid::
+ * regrid_error, :2746-2747) or has restriction disabled (do_restrict,
+ * :2749-2750); of the others every time level but the oldest is restricted,
+ * all of them when the group has only one (:2755-2756).  The selected time
+ * levels' FAB pairs form one restriction plan (execute, stats and destroy as
+ * for cx_restrict_plan_create): one launch per index type instead of one
+ * average_down per group and time level.  restricted[g] receives how many
+ * time levels of group g the plan restricts (0 if skipped): the caller then
+ * marks the ghosts and the outer boundary of those time levels invalid on
+ * the coarse level (:2821-2826).  Every FAB pair of a group must carry the
+ * group's indextype and ncomp. */
+typedef struct {
+  int indextype;       /* the group's centring, as for cx_restrict_box */
+  int ncomp;           /* the group's variables */
+  int ntimelevels;     /* time levels the group stores (0 = the newest) */
+  int do_restrict;     /* GroupData::do_restrict */
+  int is_regrid_error; /* the group is CarpetXRegrid::regrid_error */
+  int nfabs;           /* FAB pairs of one time level */
+  const cx_restrict_box_t *fabs; /* ntimelevels x nfabs, time level major */
+} cx_restrict_group_t;
+int cx_restrict_groups_plan_create(const cx_restrict_group_t *groups, int ngroups,
+                                   int *restricted, cx_restrict_plan_t *out);
+
 /* ---------------------------------------------------------------------- */
 /* Adjoints (no reference counterpart: the transposes of the above)        */
 

@@ -237,3 +237,19 @@ class RefOracle:
                                   _i3(rhi), int(ncomp))
         if rc != 0:
             raise ValueError("unknown operator")
+
+
+def restrict_selection(groups):
+    """Time levels Restrict() restricts per group (CarpetX/src/
+    schedule.cxx:2717-2837): none for the regrid error (:2746-2747) or a
+    group with do_restrict false (:2749-2750); otherwise all but the oldest,
+    all of them when the group has one (:2755-2756).  groups: dicts with
+    keys ntimelevels, do_restrict and optionally is_regrid_error."""
+    out = []
+    for g in groups:
+        if g.get("is_regrid_error", False) or not g["do_restrict"]:
+            out.append(0)
+            continue
+        n = int(g["ntimelevels"])
+        out.append(n - 1 if n > 1 else n)
+    return out

@@ -70,3 +70,46 @@ def test_gpu_restrict_plan_rejects(dev):
     with pytest.raises(cb.CxError) as e:
         cb.RestrictPlan([box])
     assert e.value.status == cb.CX_EUNSUPPORTED
+
+
+def test_gpu_restrict_groups_plan_selects_like_restrict(cx, dev):
+    """Restrict() of one level through cx_restrict_groups_plan_create: groups
+    of every kind the reference tells apart (one time level, several, the
+    regrid error, restriction disabled); the restricted time levels equal the
+    oracle's restriction bit for bit, the others keep their coarse data."""
+    import torch
+    import carpetx_b200 as cb
+    from oracle.oracle import restrict_selection
+    specs = [dict(ntimelevels=1, do_restrict=True), dict(ntimelevels=3, do_restrict=True),
+             dict(ntimelevels=2, do_restrict=False),
+             dict(ntimelevels=1, do_restrict=True, is_regrid_error=True),
+             dict(ntimelevels=2, do_restrict=True)]
+    groups = []
+    for g, sp in enumerate(specs):
+        # a group has one centring: the boxes of the first one drawn; every
+        # time level has the same boxes with its own data
+        lvl = _level(dev, 8, 1 + g % 3, 100 + g)
+        it = lvl[0]["indextype"]
+        lvl = [b for b in lvl if b["indextype"] == it]
+        tls = []
+        for tl in range(sp["ntimelevels"]):
+            tls.append([dict(b, fine=torch.randn_like(b["fine"]),
+                             crse=torch.full_like(b["crse"], 1.0 + tl)) for b in lvl])
+        groups.append(dict(sp, indextype=it, ncomp=1 + g % 3, fabs=tls))
+    before = [[[b["crse"].clone() for b in t] for t in gr["fabs"]] for gr in groups]
+    plan = cb.RestrictPlan.for_groups(groups)
+    want_n = restrict_selection(groups)
+    assert plan.restricted == want_n
+    plan.execute()
+    torch.cuda.synchronize()
+    for g, gr in enumerate(groups):
+        for tl, t in enumerate(gr["fabs"]):
+            for i, b in enumerate(t):
+                got = b["crse"].cpu().numpy()
+                ref = before[g][tl][i].cpu().numpy()
+                if tl < want_n[g]:
+                    cx.restrict(b["indextype"], b["fine"].cpu().numpy(), b["fine_lo"],
+                                b["fine_hi"], ref, b["crse_lo"], b["crse_hi"], b["reg_lo"],
+                                b["reg_hi"], b["ncomp"])
+                assert_bitwise(got, ref, f"group {g} time level {tl} FAB {i}")
+    plan.close()
