@@ -65,11 +65,13 @@ METRIC = "FP64 fine points/s, batched persistent level prolongation"
 UNIT = "fine points/s"
 L2_BYTES = 126 * 1024 * 1024
 E2E_BATCHES = 8  # box batches of the end-to-end leg's copy/transfer pipeline
-# ncu DRAM bytes per fine point of the level512 workload (the eight kernels
-# of a step, 2-component capture: 283.2 MB read + 1138.3 MB written for
-# 172,696,778 fine points; ncu flushes the L2 between launches, so the fine
-# lines still dirty in the L2 when a launch ends are written back outside it)
-TRAFFIC_PER_FINE_POINT = 1421.55e6 / 172696778
+# ncu DRAM bytes per fine point of the level512 workload's step (the eight
+# separable kernels), from a capture of the same 512 boxes with 2 components
+# instead of 24 (1/12 of the fine points) with --cache-control none, so that
+# write-backs of lines a launch dirtied count in the launches that follow:
+# 579,898,112 B read + 2,769,938,688 B written over 16 launches (two steps)
+# for 172,696,778 fine points per step; the traffic grows with the fine points
+TRAFFIC_PER_FINE_POINT = (579898112 + 2769938688) / 2 / 172696778
 
 
 def parse():
@@ -725,19 +727,30 @@ def main():
             if rc:
                 raise RuntimeError(L.cx_last_error().decode())
 
+    # the per-box launches are captured once as a CUDA graph and replayed,
+    # so the figure is the device-side cost of the reference's launch
+    # granularity, without this script's per-call host overhead
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ms_pb, per_box_value = None, None
     if args.per_box_steps > 0:
-        per_box_step()
+        with torch.cuda.stream(stream):
+            per_box_step()
+        torch.cuda.synchronize()
+        g_pb = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g_pb, stream=stream):
+            per_box_step()
+        g_pb.replay()
         torch.cuda.synchronize()
         barrier()
-        e0.record(stream)
-        for _ in range(args.per_box_steps):
-            per_box_step()
-        e1.record(stream)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(args.per_box_steps):
+                g_pb.replay()
+            e1.record(stream)
         barrier()
         ms_pb = max_over_ranks(e0.elapsed_time(e1)) / args.per_box_steps
         per_box_value = total_fine / (ms_pb / 1e3)
+        del g_pb
 
     # end to end through the C ABI with host buffers: every step copies all
     # coarse data in from pinned host memory and all fine data out.  The
@@ -830,6 +843,7 @@ def main():
         "gpu_launches": args.steps * st["launches"],
         "per_box": {"value": per_box_value, "unit": UNIT, "ms_per_step": ms_pb,
                     "launches_per_step": len(calls),
+                    "timing": "one CUDA graph of the per-box launches, replayed",
                     "batched_speedup": value / per_box_value if per_box_value else None},
         "e2e": {"value": e2e_value, "unit": UNIT, "ms_per_step": ms_e2e,
                 "h2d_bytes_per_step": 8 * ctot, "d2h_bytes_per_step": 8 * ftot},

@@ -172,6 +172,8 @@ def lib():
         L.cx_restrict_groups_plan_create.argtypes = [ctypes.POINTER(CxRestrictGroup), _I,
                                                      ctypes.POINTER(_I), ctypes.POINTER(_VP)]
         L.cx_debug_set_wait_limit.argtypes = [ctypes.c_longlong]
+        L.cx_debug_stream_kind.argtypes = [ctypes.c_int32]
+        L.cx_debug_set_stream_schedule.argtypes = [_I, _I, _I]
         _lib = L
     return _lib
 

@@ -194,6 +194,7 @@ struct cx_level_plan {
   // items of kernel group g: [group_off[g], group_off[g + 1]) of d_tiles
   int group_off[kStrGroups + 1] = {};
   int group_grid[kStrGroups] = {};
+  int group_sched[kStrGroups] = {}; // streaming groups: schedule picked at creation
   int64_t nfine = 0, bytes = 0;
   // adjoint plan: execute computes crse = P^T fine for every box; coarse
   // boxes whose region is empty are zeroed (pointer, bytes)
@@ -273,7 +274,10 @@ int cx_prolong_box_diag(cx_op_t op, const double *crse, const int crse_lo[3], co
   // one box per launch: spread it over the GPU (z chunks sized by the grid of
   // the 256-thread variant, whichever CTA size the box then takes)
   if (use_stream(op, per_group))
-    stream_tiling(b, stream_level_grid(stream_group_of(b.kind[0], b.kind[1], b.kind[2])));
+    {
+      const int g = stream_group_of(b.kind[0], b.kind[1], b.kind[2]);
+      stream_tiling(b, stream_level_grid(g, stream_sched(g)));
+    }
   if (use_stream(op, per_group) && !shifts && !fallback)
     return cuda_status(launch_stream_box(b, s), "prolongation launch");
   if (use_stream(op, per_group)) {
@@ -397,8 +401,11 @@ int cx_level_plan_create(const cx_box_t *boxes, int nboxes, int per_group, cx_le
     return fail(e == cudaErrorMemoryAllocation ? CX_ENOMEM : CX_ECUDA, "level plan: %s",
                 cudaGetErrorString(e));
   }
-  for (int g = 0; g < kStrGroups; ++g)
-    p->group_grid[g] = p->group_off[g + 1] > p->group_off[g] ? stream_level_grid(g) : 0;
+  for (int g = 0; g < kStrGroups; ++g) {
+    p->group_sched[g] = stream_sched(g);
+    p->group_grid[g] =
+        p->group_off[g + 1] > p->group_off[g] ? stream_level_grid(g, p->group_sched[g]) : 0;
+  }
   *out = p;
   return CX_OK;
 }
@@ -553,7 +560,8 @@ int cx_level_plan_execute(cx_level_plan_t p, cx_stream_t stream) {
     const int g = (i + kStrKinds) % kStrGroups;
     const int n = p->group_off[g + 1] - p->group_off[g];
     if (n > 0) {
-      if (int e = cuda_status(launch_stream_level(g, p->d_boxes, p->d_tiles + p->group_off[g], n,
+      if (int e = cuda_status(launch_stream_level(g, p->group_sched[g], p->d_boxes,
+                                                  p->d_tiles + p->group_off[g], n,
                                                   p->group_grid[g], p->d_counters + g, s,
                                                   after_level),
                               "level launch"))
@@ -582,6 +590,20 @@ int cx_check_device(void) {
     return fail(CX_ECUDA, "reading the device wait flag failed");
   if (t > 0)
     return fail(CX_ETIMEOUT, "a bounded device wait gave up (its results are not valid)");
+  return CX_OK;
+}
+
+int cx_debug_stream_kind(cx_op_t op) {
+  if (!valid_op(op))
+    return fail(CX_EINVAL, "invalid operator handle %d", (int)op);
+  if (!use_stream(op, 0))
+    return -1;
+  return stream_group_of(op_kind(op, 0), op_kind(op, 1), op_kind(op, 2));
+}
+
+int cx_debug_set_stream_schedule(int kind, int sched, int maxz) {
+  if (stream_set_schedule(kind, sched, maxz) != 0)
+    return fail(CX_EINVAL, "kind %d, schedule %d or z cap %d out of range", kind, sched, maxz);
   return CX_OK;
 }
 

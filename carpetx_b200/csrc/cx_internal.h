@@ -81,16 +81,25 @@ int stream_pair_of(int kx, int ky, int kz);
 int stream_group_of(int kx, int ky, int kz);
 constexpr int kStrKinds = 136;            // instantiations per CTA size (8 x kStreamPairs)
 constexpr int kStrGroups = 2 * kStrKinds; // level groups: both CTA sizes
-// Level launch of the items of one instantiation; d_items holds only items
-// of boxes served by that group, sorted by cost; d_counter: one int, zero
-// before the launch (the CTAs take items from it).  after_level: the launch
-// directly follows another level launch of the same transfer on s (boxes
-// disjoint), and may start while that one finishes (programmatic dependent
-// launch).
-cudaError_t launch_stream_level(int group, const BoxDesc *d_boxes,
+// Schedule of a level group's kernel (0 or 1; the 128-thread groups have
+// 0): a setting of stream_set_schedule, else the tuned table
+// (stream_tuned.h), else the default rule.  stream_maxz: the z-chunk cap of
+// an instantiation (fine points, even, 16..128), chosen the same way.
+int stream_sched(int group);
+int stream_maxz(int kind);
+// Settings for the tuner (cx_debug_set_stream_schedule): instantiation kind
+// (-1: all), schedule (-1: none), z-chunk cap (0: none); -1 if invalid.
+int stream_set_schedule(int kind, int sched, int maxz);
+// Level launch of the items of one instantiation with a schedule; d_items
+// holds only items of boxes served by that group, sorted by cost;
+// d_counter: one int, zero before the launch (the CTAs take items from it).
+// after_level: the launch directly follows another level launch of the same
+// transfer on s (boxes disjoint), and may start while that one finishes
+// (programmatic dependent launch).
+cudaError_t launch_stream_level(int group, int sched, const BoxDesc *d_boxes,
                                 const TileRef *d_items, int nitems, int grid,
                                 int *d_counter, cudaStream_t s, bool after_level);
-int stream_level_grid(int group);
+int stream_level_grid(int group, int sched);
 // Fills the streaming-kernel tiling of a box (tbase, ntile, zchunk, xcw,
 // npr, upi); min_items > 0 shortens the z chunks of a box launched alone so
 // that it spreads over at least that many CTAs where it can.

@@ -175,7 +175,7 @@ extern "C" int cx_level_execute_noalloc(const cx_box_t *boxes, int nboxes, int p
   for (int g = 0; e == cudaSuccess && g < kStrGroups; ++g) {
     const int n = off[g + 1] - off[g];
     if (n > 0)
-      e = launch_stream_level(g, dev->boxes, dev->items + off[g], n, stream_level_grid(g),
+      e = launch_stream_level(g, stream_sched(g), dev->boxes, dev->items + off[g], n, stream_level_grid(g, stream_sched(g)),
                               dev->counters + g, s, false);
   }
   for (int id = 0; e == cudaSuccess && id < nb; ++id)

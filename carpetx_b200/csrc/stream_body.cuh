@@ -372,7 +372,7 @@ __device__ __forceinline__ void load_plane(const Item &it, const int64_t *rlen, 
 // phase parity (seq / NRING) & 1, x-pass buffer seq & 1.  Returns false if a
 // bounded wait gave up (every thread alike): the copies still in flight
 // have landed (bounded) when it returns.
-template <class KV, class KC, int CM>
+template <class KV, class KC, int CM, int SCHED>
 __device__ __forceinline__ bool stream_item(Shared &sh, const Item &it, uint32_t &seq,
                                             long long limit) {
   using KX = typename Kinds<KV, KC, CM>::KX;
@@ -398,13 +398,31 @@ __device__ __forceinline__ bool stream_item(Shared &sh, const Item &it, uint32_t
         wait_plane_slow(&sh.full[slot], (seq / NRING) & 1u, &sh.fail, limit);
       const double *S = sh.s0[slot] + ((c - it.clo_z) & it.cpl1);
       double *X = sh.xs[seq & 1];
+      if constexpr (SCHED == 1) {
+        // a rolled loop: one copy of the task body per unrolled plane keeps
+        // the kernel's code small (with three CTAs per SM, instruction fetch
+        // stalls otherwise cost more than the loop)
+#pragma unroll 1
+        for (int k = 0; k < it.nxt; ++k) {
+          int src = it.xt_src[0], dst = it.xt_dst[0];
 #pragma unroll
-      for (int k = 0; k < XTMAX; ++k) {
-        if (k >= it.nxt)
-          break;
-        if (it.xt_src[k] < 0)
-          continue;
-        xtask<KX>(S + it.xt_src[k], X + it.xt_dst[k]);
+          for (int kk = 1; kk < XTMAX; ++kk)
+            if (k == kk) {
+              src = it.xt_src[kk];
+              dst = it.xt_dst[kk];
+            }
+          if (src >= 0)
+            xtask<KX>(S + src, X + dst);
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < XTMAX; ++k) {
+          if (k >= it.nxt)
+            break;
+          if (it.xt_src[k] < 0)
+            continue;
+          xtask<KX>(S + it.xt_src[k], X + it.xt_dst[k]);
+        }
       }
       // every thread has read the slot and written its x results (the
       // other x buffer's readers, plane c - 1, are past this barrier too)
@@ -463,7 +481,7 @@ __device__ __forceinline__ bool stream_item(Shared &sh, const Item &it, uint32_t
   return true;
 }
 
-template <class KV, class KC, int CM>
+template <class KV, class KC, int CM, int SCHED>
 __device__ __forceinline__ bool run_item(Shared &sh, const BoxDesc &b, int xchunk, int ublock,
                                          int zchunk, int comp, uint32_t &seq, long long limit) {
   Item it;
@@ -472,7 +490,7 @@ __device__ __forceinline__ bool run_item(Shared &sh, const BoxDesc &b, int xchun
                  it, sh.rlen))
     return true;
   __syncthreads(); // rlen
-  return stream_item<KV, KC, CM>(sh, it, seq, limit);
+  return stream_item<KV, KC, CM, SCHED>(sh, it, seq, limit);
 }
 
 __device__ __forceinline__ void init_shared(Shared &sh) {
@@ -494,11 +512,19 @@ static_assert(BOX_WORDS <= NTS, "one thread per descriptor word");
 // counter;
 // the descriptors of the next item are loaded into registers while the
 // current item streams, so no global-memory latency sits between two items.
-// Two CTAs of 256 threads (four of 128) per SM, at most 128 registers,
-// except the order-7 z kinds whose register ring (8 or 9 planes) needs more:
-// half as many.
-template <class KV, class KC, int CM>
-__global__ void __launch_bounds__(NTS, (Kinds<KV, KC, CM>::ZHI - Kinds<KV, KC, CM>::ZLO >= 7 ? 1 : 2) * (256 / NTS))
+// Schedules (SCHED) of the 256-thread kernel, picked per instantiation by
+// the tuned table (stream_tuned.h, written by carpetx_b200/tune.py):
+//   0: two CTAs per SM (at most 128 registers), x-task loop unrolled;
+//   1: three CTAs per SM (at most 80 registers, a few words may spill),
+//      x-task loop rolled (a smaller body).
+// The order-7 z kinds, whose register ring holds 8 or 9 planes, run one CTA
+// per SM in both; the 128-thread variant has one schedule, four CTAs per SM
+// (two for the order-7 z kinds).
+template <int DZ, int SCHED> struct StreamOcc {
+  static constexpr int value = NTS == 256 ? (DZ >= 7 ? 1 : SCHED == 1 ? 3 : 2) : (DZ >= 7 ? 2 : 4);
+};
+template <class KV, class KC, int CM, int SCHED>
+__global__ void __launch_bounds__(NTS, StreamOcc<Kinds<KV, KC, CM>::ZHI - Kinds<KV, KC, CM>::ZLO, SCHED>::value)
     stream_kernel(const BoxDesc b, const BoxDesc *__restrict__ boxes,
                   const TileRef *__restrict__ items, int nitems, int *__restrict__ counter) {
   extern __shared__ __align__(16) unsigned char smem_raw[]; // sizeof(Shared) bytes
@@ -515,7 +541,7 @@ __global__ void __launch_bounds__(NTS, (Kinds<KV, KC, CM>::ZHI - Kinds<KV, KC, C
       r /= b.ntile[1];
       const int zchunk = r % b.ntile[2];
       const int comp = r / b.ntile[2];
-      if (!run_item<KV, KC, CM>(sh, b, xchunk, ublock, zchunk, comp, seq, limit))
+      if (!run_item<KV, KC, CM, SCHED>(sh, b, xchunk, ublock, zchunk, comp, seq, limit))
         return;
     }
     return;
@@ -561,7 +587,8 @@ __global__ void __launch_bounds__(NTS, (Kinds<KV, KC, CM>::ZHI - Kinds<KV, KC, C
     TileRef t_next2 = t_next;
     if (nxt2 < nitems)
       t_next2 = items[nxt2]; // work-list entry of the item after next
-    if (!run_item<KV, KC, CM>(sh, box_s, t_cur.tx, t_cur.ty, t_cur.tz, t_cur.comp, seq, limit) ||
+    if (!run_item<KV, KC, CM, SCHED>(sh, box_s, t_cur.tx, t_cur.ty, t_cur.tz, t_cur.comp, seq,
+                                     limit) ||
         nxt >= nitems) {
       asm volatile("griddepcontrol.wait;" ::: "memory");
       break;

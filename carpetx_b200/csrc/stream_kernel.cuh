@@ -77,5 +77,21 @@ static_assert(small::NU == kStrSmallUnits, "the small variant holds a small box'
 
 using KernelFn = void (*)(const BoxDesc, const BoxDesc *, const TileRef *, int, int *);
 
+// The kernel of an instantiation for a CTA size and schedule (the 128-thread
+// variant and the order-7 z kinds have schedule 0 only).
+template <class V, class C, int CM> KernelFn pick_kernel(bool small_cta, int sched) {
+  if (small_cta)
+    return small::stream_kernel<V, C, CM, 0>;
+  if constexpr (big::Kinds<V, C, CM>::ZHI - big::Kinds<V, C, CM>::ZLO < 7) {
+    if (sched == 1)
+      return big::stream_kernel<V, C, CM, 1>;
+  }
+  return big::stream_kernel<V, C, CM, 0>;
+}
+// Whether an instantiation's 256-thread kernel has schedule 1.
+template <class V, class C, int CM> constexpr bool has_sched1() {
+  return big::Kinds<V, C, CM>::ZHI - big::Kinds<V, C, CM>::ZLO < 7;
+}
+
 } // namespace stream
 } // namespace cxb

@@ -5,17 +5,18 @@
 
 #include "stream_kernel.cuh"
 #include "stream_pairs.h"
+#include "stream_tuned.h"
 
 namespace cxb {
 namespace stream {
-KernelFn kernel_part0(int group, bool small_cta);
-KernelFn kernel_part1(int group, bool small_cta);
-KernelFn kernel_part2(int group, bool small_cta);
-KernelFn kernel_part3(int group, bool small_cta);
-KernelFn kernel_part4(int group, bool small_cta);
-KernelFn kernel_part5(int group, bool small_cta);
-KernelFn kernel_part6(int group, bool small_cta);
-KernelFn kernel_part7(int group, bool small_cta);
+KernelFn kernel_part0(int group, bool small_cta, int sched);
+KernelFn kernel_part1(int group, bool small_cta, int sched);
+KernelFn kernel_part2(int group, bool small_cta, int sched);
+KernelFn kernel_part3(int group, bool small_cta, int sched);
+KernelFn kernel_part4(int group, bool small_cta, int sched);
+KernelFn kernel_part5(int group, bool small_cta, int sched);
+KernelFn kernel_part6(int group, bool small_cta, int sched);
+KernelFn kernel_part7(int group, bool small_cta, int sched);
 int str_set_wait_limit_part0(long long);
 int str_set_wait_limit_part1(long long);
 int str_set_wait_limit_part2(long long);
@@ -34,11 +35,42 @@ int str_timeout_part6();
 int str_timeout_part7();
 
 namespace {
-// Per device (cache_device()): dynamic shared memory allowed per group
-// (the attribute applies per device), SM count, persistent grid per group.
-std::atomic<bool> g_attr_set[kMaxDevices][kStrGroups];
+// Per device (cache_device()) and schedule: dynamic shared memory allowed
+// per group (the attribute applies per device), SM count, persistent grid
+// per group.
+std::atomic<bool> g_attr_set[kMaxDevices][kStrGroups][2];
 std::atomic<int> g_sms[kMaxDevices];
-std::atomic<int> g_grid[kMaxDevices][kStrGroups];
+std::atomic<int> g_grid[kMaxDevices][kStrGroups][2];
+// Settings of cx_debug_set_stream_schedule per instantiation: schedule
+// (-1: none) and z-chunk cap (0: none).
+std::atomic<int> g_sched_set[kStrKinds];
+std::atomic<int> g_maxz_set[kStrKinds];
+struct SetInit {
+  SetInit() {
+    for (int k = 0; k < kStrKinds; ++k) {
+      g_sched_set[k].store(-1);
+      g_maxz_set[k].store(0);
+    }
+  }
+} g_set_init;
+
+// Per instantiation: whether its 256-thread kernel has schedule 1, and the
+// spread (RHI - RLO) of its z kind.
+constexpr bool kHasSched1[kStrKinds] = {
+#define CXB_HS(I, V, C, KVI, KCI)                                              \
+  has_sched1<V, C, 0>(), has_sched1<V, C, 1>(), has_sched1<V, C, 2>(),         \
+      has_sched1<V, C, 3>(), has_sched1<V, C, 4>(), has_sched1<V, C, 5>(),     \
+      has_sched1<V, C, 6>(), has_sched1<V, C, 7>(),
+    CXB_STREAM_PAIRS(CXB_HS)
+#undef CXB_HS
+};
+constexpr int kZSpread[kStrKinds] = {
+#define CXB_ZS(I, V, C, KVI, KCI)                                              \
+  V::RHI - V::RLO, C::RHI - C::RLO, V::RHI - V::RLO, C::RHI - C::RLO,          \
+      V::RHI - V::RLO, C::RHI - C::RLO, V::RHI - V::RLO, C::RHI - C::RLO,
+    CXB_STREAM_PAIRS(CXB_ZS)
+#undef CXB_ZS
+};
 
 // Threads and dynamic shared memory of a level group's CTA size.
 int threads_of(int group) { return group >= kStrKinds ? small::NTS : big::NTS; }
@@ -47,21 +79,22 @@ size_t smem_of(int group) {
 }
 
 // Kernel of a level group (instantiation + kStrKinds for the 128-thread
-// variant); the first lookup on a device allows its dynamic shared memory,
-// which may exceed the 48 KB default.
-KernelFn kernel_for(int group) {
+// variant) and schedule; the first lookup on a device allows its dynamic
+// shared memory, which may exceed the 48 KB default.
+KernelFn kernel_for(int group, int sched) {
   if (group < 0 || group >= kStrGroups)
     return nullptr;
-  static KernelFn (*const parts[kStreamParts])(int, bool) = {
+  static KernelFn (*const parts[kStreamParts])(int, bool, int) = {
       kernel_part0, kernel_part1, kernel_part2, kernel_part3,
       kernel_part4, kernel_part5, kernel_part6, kernel_part7};
   const int kind = group % kStrKinds;
-  KernelFn k = parts[kind % kStreamParts](kind, group >= kStrKinds);
+  const int sc = group >= kStrKinds ? 0 : sched;
+  KernelFn k = parts[kind % kStreamParts](kind, group >= kStrKinds, sc);
   const int dev = cache_device();
-  if (k && (dev < 0 || !g_attr_set[dev][group].load())) {
+  if (k && (dev < 0 || !g_attr_set[dev][group][sc].load())) {
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_of(group));
     if (dev >= 0)
-      g_attr_set[dev][group].store(true);
+      g_attr_set[dev][group][sc].store(true);
   }
   return k;
 }
@@ -79,6 +112,45 @@ int sms() {
 }
 } // namespace
 } // namespace stream
+
+int stream_sched(int group) {
+  using namespace stream;
+  if (group < 0 || group >= kStrKinds)
+    return 0; // the 128-thread variant (or none)
+  if (!kHasSched1[group])
+    return 0;
+  const int set = g_sched_set[group].load();
+  if (set >= 0)
+    return set;
+  if (kStreamTuned[group].sched >= 0)
+    return kStreamTuned[group].sched;
+  // untuned: three CTAs per SM for z spreads of 4 (the order-3 conservative
+  // and order-3/4 polynomial cell-centred z kinds), measured faster on the
+  // mixed 512-box level; two elsewhere
+  return kZSpread[group] == 4 ? 1 : 0;
+}
+
+int stream_maxz(int kind) {
+  using namespace stream;
+  if (kind < 0 || kind >= kStrKinds)
+    return 128;
+  const int set = g_maxz_set[kind].load();
+  if (set > 0)
+    return set;
+  return kStreamTuned[kind].maxz > 0 ? kStreamTuned[kind].maxz : 128;
+}
+
+int stream_set_schedule(int kind, int sched, int maxz) {
+  using namespace stream;
+  if (kind < -1 || kind >= kStrKinds || sched < -1 || sched > 1 || maxz < 0 || maxz > 128 ||
+      (maxz > 0 && (maxz < 16 || (maxz & 1))))
+    return -1;
+  for (int k = kind < 0 ? 0 : kind; k < (kind < 0 ? kStrKinds : kind + 1); ++k) {
+    g_sched_set[k].store(sched);
+    g_maxz_set[k].store(maxz);
+  }
+  return 0;
+}
 
 int stream_set_wait_limit(long long cycles) {
   using namespace stream;
@@ -165,13 +237,13 @@ void stream_tiling(BoxDesc &b, int min_items) {
   const int nu = b.scta ? small::NU : big::NU;
   b.upi = nu < PRMAX * b.xcw ? nu : PRMAX * b.xcw;
   b.ntile[1] = (b.npr * b.xcw + b.upi - 1) / b.upi;
-  // fine z per item: whole columns up to 128 fine points, else near-equal
-  // even chunks of at most 128 (the z halo and the pipeline start cost extra
-  // planes per chunk); shorter chunks (down to 16) when the box alone must
-  // fill min_items CTAs
+  // fine z per item: whole columns up to the instantiation's cap (tuned, 128
+  // by default), else near-equal even chunks of at most the cap (the z halo
+  // and the pipeline start cost extra planes per chunk); shorter chunks
+  // (down to 16) when the box alone must fill min_items CTAs
   const int E = b.rhi[2] - b.tbase[2] + 1;
   const int64_t xy_items = (int64_t)b.ntile[0] * b.ntile[1] * b.ncomp;
-  int maxz = 128;
+  int maxz = stream_maxz(stream_group_of(b.kind[0], b.kind[1], b.kind[2]));
   while (maxz > 16 && xy_items * ((E + maxz - 1) / maxz) < min_items)
     maxz /= 2;
   const int nch = (E + maxz - 1) / maxz;
@@ -181,19 +253,20 @@ void stream_tiling(BoxDesc &b, int min_items) {
   b.ntile[2] = (E + zc - 1) / zc;
 }
 
-int stream_level_grid(int group) {
+int stream_level_grid(int group, int sched) {
   using namespace stream;
-  KernelFn k = kernel_for(group);
+  const int sc = group >= kStrKinds ? 0 : (sched ? 1 : 0);
+  KernelFn k = kernel_for(group, sc);
   if (!k)
     return 0;
   const int dev = cache_device();
-  if (dev >= 0 && g_grid[dev][group].load())
-    return g_grid[dev][group].load();
+  if (dev >= 0 && g_grid[dev][group][sc].load())
+    return g_grid[dev][group][sc].load();
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads_of(group), smem_of(group));
   const int grid = sms() * (per_sm > 0 ? per_sm : 1);
   if (dev >= 0)
-    g_grid[dev][group].store(grid);
+    g_grid[dev][group][sc].store(grid);
   return grid;
 }
 
@@ -208,22 +281,23 @@ cudaError_t launch_stream_box(const BoxDesc &b, cudaStream_t s) {
   if (kind < 0)
     return cudaErrorInvalidValue;
   const int group = kind + (b.scta ? kStrKinds : 0);
-  KernelFn k = kernel_for(group);
+  const int sched = stream_sched(group);
+  KernelFn k = kernel_for(group, sched);
   if (!k)
     return cudaErrorInvalidValue;
   const int n = (int)n64;
-  const int cap = stream_level_grid(group);
+  const int cap = stream_level_grid(group, sched);
   k<<<n < cap ? n : cap, threads_of(group), smem_of(group), s>>>(b, nullptr, nullptr, n, nullptr);
   return cudaGetLastError();
 }
 
-cudaError_t launch_stream_level(int group, const BoxDesc *d_boxes, const TileRef *d_items,
-                                int nitems, int grid, int *d_counter, cudaStream_t s,
-                                bool after_level) {
+cudaError_t launch_stream_level(int group, int sched, const BoxDesc *d_boxes,
+                                const TileRef *d_items, int nitems, int grid, int *d_counter,
+                                cudaStream_t s, bool after_level) {
   using namespace stream;
   if (nitems <= 0)
     return cudaSuccess;
-  KernelFn k = kernel_for(group);
+  KernelFn k = kernel_for(group, sched);
   if (!k)
     return cudaErrorInvalidValue;
   BoxDesc unused{};

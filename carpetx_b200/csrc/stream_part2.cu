@@ -8,11 +8,11 @@
 namespace cxb {
 namespace stream {
 
-KernelFn kernel_part2(int group, bool small_cta) {
+KernelFn kernel_part2(int group, bool small_cta, int sched) {
   switch (group) {
 #define CXB_PAIR_CASE(I, V, C, KVI, KCI)                                       \
   case kStreamParts * I + 2:                                                   \
-    return small_cta ? small::stream_kernel<V, C, 2> : big::stream_kernel<V, C, 2>;
+    return pick_kernel<V, C, 2>(small_cta, sched);
     CXB_STREAM_PAIRS(CXB_PAIR_CASE)
 #undef CXB_PAIR_CASE
   default:

@@ -64,6 +64,21 @@ int cx_check_device(void);
  * reference (its kernels never wait). */
 int cx_debug_set_wait_limit(long long cycles);
 
+/* Tuning entry points (no counterpart in the reference: its kernels have
+ * no schedules).  The separable operators run on one streaming-kernel
+ * instantiation per stencil pair and centring; cx_debug_stream_kind
+ * returns an operator's instantiation index (0..135; -1 for an operator
+ * the streaming kernels do not serve, e.g. ENO).  Each instantiation has a
+ * schedule (0: two CTAs per SM; 1: three CTAs per SM with a smaller loop
+ * body) and a cap on the fine z points of a work item (even, 16..128),
+ * taken from the tuned table the library was built with (written by
+ * carpetx_b200/tune.py) unless cx_debug_set_stream_schedule sets them for
+ * this process: kind -1 sets every instantiation, schedule -1 and cap 0
+ * restore the table.  Plans take the setting in force when they are
+ * created; results do not depend on it. */
+int cx_debug_stream_kind(cx_op_t op);
+int cx_debug_set_stream_schedule(int kind, int sched, int maxz);
+
 /* Human-readable name of a status code. */
 const char *cx_status_string(int status);
 /* Text of the most recent failure on this thread ("" if none). */
