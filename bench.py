@@ -95,6 +95,8 @@ def parse():
                    help="executions of the halo-exchange leg (0: skip)")
     p.add_argument("--boundary-steps", type=int, default=5,
                    help="executions of the boundary-condition leg (0: skip)")
+    p.add_argument("--tune-steps", type=int, default=5,
+                   help="steps of the tuned / untuned schedule comparison (0: skip)")
     p.add_argument("--boxes", type=int, default=512, help="level512: number of boxes")
     p.add_argument("--ncomp", type=int, default=24, help="level512: variables per box")
     return p.parse_args()
@@ -294,12 +296,21 @@ def limited_leg(args, cb, torch, dev, max_over_ranks, barrier):
             for bid, clo, chi, flo, fhi in sboxes]
     fine = [torch.empty((nc,) + box_shape(flo, fhi), dtype=torch.float64, device=dev)
             for bid, clo, chi, flo, fhi in sboxes]
-    for typ, order in (("eno", 3), ("minmod", 1)):
+    L = cb.lib()
+    for typ, order, untuned in (("eno", 3, False), ("minmod", 1, False), ("minmod", 1, True)):
         op = cb.Op(typ, order, 7)
         boxes = [dict(op=op, ncomp=nc, crse=c, crse_lo=clo, crse_hi=chi, fine=f, fine_lo=flo,
                       fine_hi=fhi, reg_lo=flo, reg_hi=fhi)
                  for (bid, clo, chi, flo, fhi), c, f in zip(sboxes, crse, fine)]
-        plan = cb.LevelPlan(boxes)
+        if untuned:
+            # the plan as the untuned schedule builds it (every instantiation
+            # schedule 0, cap 128), against the tuned table
+            L.cx_debug_set_stream_schedule(-1, 0, 128)
+            plan = cb.LevelPlan(boxes)
+            L.cx_debug_set_stream_schedule(-1, -1, 0)
+            typ = "minmod_untuned"
+        else:
+            plan = cb.LevelPlan(boxes)
         for _ in range(2):
             plan.execute()
         barrier()
@@ -705,6 +716,36 @@ def main():
     ms_step = ms_total / args.steps
     value = total_fine * args.steps / (ms_total / 1e3)
 
+    # the same level under the untuned schedule (every instantiation
+    # schedule 0 with a z-chunk cap of 128) against the tuned table that
+    # plan above uses (csrc/stream_tuned.h, written by carpetx_b200/tune.py)
+    tuning = None
+    if args.tune_steps > 0:
+        L0 = cb.lib()
+        L0.cx_debug_set_stream_schedule(-1, 0, 128)
+        plan_u = cb.LevelPlan(lb)
+        L0.cx_debug_set_stream_schedule(-1, -1, 0)
+        with torch.cuda.stream(stream):
+            for _ in range(2):
+                plan_u.execute(stream)
+                plan.execute(stream)
+        res_t = {}
+        for name, pl in (("untuned", plan_u), ("tuned", plan)):
+            barrier()
+            e0t, e1t = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                e0t.record(stream)
+                for _ in range(args.tune_steps):
+                    pl.execute(stream)
+                e1t.record(stream)
+            barrier()
+            res_t[name] = max_over_ranks(e0t.elapsed_time(e1t)) / args.tune_steps
+        plan_u.close()
+        tuning = {"workload": "the level of this line, eager plan executions",
+                  "tuned_ms": res_t["tuned"], "untuned_ms": res_t["untuned"],
+                  "speedup": res_t["untuned"] / res_t["tuned"],
+                  "table": "carpetx_b200/csrc/stream_tuned.h"}
+
     # the same work launched once per box per component (our kernel)
     L = cb.lib()
     I3 = ctypes.c_int * 3
@@ -857,6 +898,7 @@ def main():
         "adjoint": adjoint,
         "restriction": restriction,
         "limited": limited,
+        "tuning": tuning,
         "boundary": boundary,
         "halo": halo,
     }
