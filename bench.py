@@ -95,6 +95,8 @@ def parse():
                    help="executions of the halo-exchange leg (0: skip)")
     p.add_argument("--boundary-steps", type=int, default=5,
                    help="executions of the boundary-condition leg (0: skip)")
+    p.add_argument("--sync-steps", type=int, default=10,
+                   help="ghost-shell and sync-chain steps (0: skip)")
     p.add_argument("--tune-steps", type=int, default=5,
                    help="steps of the tuned / untuned schedule comparison (0: skip)")
     p.add_argument("--boxes", type=int, default=512, help="level512: number of boxes")
@@ -326,6 +328,145 @@ def limited_leg(args, cb, torch, dev, max_over_ranks, barrier):
         out[f"{typ}_launches"] = plan.stats()["launches"]
         plan.close()
         del boxes
+    return out
+
+
+def sync_leg(args, cb, torch, dev, max_over_ranks, barrier, peak):
+    """The per-step sync's prolongation on ghost shells, and the whole sync.
+
+    ghost_shell: every box of the mixed 512-box level as a fine FAB with 3
+    ghost cells per side whose whole shell is uncovered (the boxes do not
+    touch), 24 variables, the level512 operators; the shell is the FAB minus
+    its valid box, six slabs 3 fine points deep, prolongated from the box's
+    coarse FAB through one level plan, against one launch per slab.
+
+    sync_chain: the six steps of carpetx_b200.sync.SyncChain (FillBoundary,
+    coarse-patch gather, coarse boundary conditions, prolongation of the
+    fine patches, scatter, fine boundary conditions) on a cell-centred coarse
+    level of 128^3 cells in 64 FABs of 32^3 and a fine level over its lower
+    corner octant, 256^3 ... 128^3 fine cells in 64 FABs of 32^3, 3 ghosts,
+    16 variables (the boundary conditions take at most 16), hermite order 3;
+    replayed as one CUDA graph."""
+    from carpetx_b200.sync import SyncChain, subtract, tiled_fabs
+    from carpetx_b200.workloads import boundary_spec, mixed_level_boxes
+    out = {}
+    nc, ng = args.ncomp, 3
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(args.seed + 7)
+    # ghost shells of the level512 boxes
+    recs, ctot, ftot = [], 0, 0
+    for it, clo0, chi0, flo, fhi in mixed_level_boxes(args.seed, nboxes=args.boxes):
+        typ, order = ("interpolate", 5) if it == 0 else ("hermite", 3)
+        op = cb.Op(typ, order, it)
+        glo = tuple(flo[d] - ng for d in range(3))
+        ghi = tuple(fhi[d] + ng for d in range(3))
+        clo, chi = op.coarse_box(glo, ghi)
+        recs.append((op, clo, chi, glo, ghi, subtract((glo, ghi), (flo, fhi)), ctot, ftot))
+        ctot += nc * npts(clo, chi)
+        ftot += nc * npts(glo, ghi)
+    crse = torch.empty(ctot, dtype=torch.float64, device=dev)
+    crse.normal_(generator=gen)
+    fine = torch.zeros(ftot, dtype=torch.float64, device=dev)
+    boxes, calls = [], []
+    L = cb.lib()
+    I3 = ctypes.c_int * 3
+    stream = torch.cuda.Stream(device=dev)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    shell_pts = 0
+    for op, clo, chi, glo, ghi, slabs, co, fo in recs:
+        c = crse[co:co + nc * npts(clo, chi)].view((nc,) + box_shape(clo, chi))
+        f = fine[fo:fo + nc * npts(glo, ghi)].view((nc,) + box_shape(glo, ghi))
+        for rlo, rhi in slabs:
+            boxes.append(dict(op=op, ncomp=nc, crse=c, crse_lo=clo, crse_hi=chi, fine=f,
+                              fine_lo=glo, fine_hi=ghi, reg_lo=rlo, reg_hi=rhi))
+            calls.append((op.handle, ctypes.c_void_p(c.data_ptr()), I3(*clo), I3(*chi),
+                          ctypes.c_void_p(f.data_ptr()), I3(*glo), I3(*ghi), I3(*rlo), I3(*rhi)))
+            shell_pts += nc * npts(rlo, rhi)
+    plan = cb.LevelPlan(boxes)
+    st = plan.stats()
+
+    def timed_graph(fn, steps):
+        with torch.cuda.stream(stream):
+            fn()
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            fn()
+        for _ in range(2):
+            g.replay()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(steps):
+                g.replay()
+            e1.record(stream)
+        barrier()
+        del g
+        return max_over_ranks(e0.elapsed_time(e1)) / steps
+
+    def per_slab():
+        for c in calls:
+            rc = L.cx_prolong_box(*c, nc, 0, sp)
+            if rc:
+                raise RuntimeError(L.cx_last_error().decode())
+
+    ms = timed_graph(lambda: plan.execute(stream), args.sync_steps)
+    ms_pb = timed_graph(per_slab, max(1, args.sync_steps // 5))
+    out["ghost_shell"] = {
+        "workload": f"{args.boxes} boxes of the mixed level as fine FABs with {ng} ghosts per side, "
+                    f"the whole shell uncovered (six slabs {ng} deep per box), {nc} vars, "
+                    "interpolate o5 VVV / hermite o3 VVC,VCC,CCC; one level plan, graph replay",
+        "regions": len(boxes), "fine_points": shell_pts, "bytes": st["bytes"], "ms": ms,
+        "fine_pts_per_s": shell_pts / (ms / 1e3),
+        "achieved_gbs": st["bytes"] / (ms / 1e3) / 1e9,
+        "frac_of_peak": st["bytes"] / (ms / 1e3) / 1e9 / peak, "launches": st["launches"],
+        "per_region_ms": ms_pb, "per_region_launches": len(calls), "batched_speedup": ms_pb / ms}
+    plan.close()
+    del boxes, calls, crse, fine
+    torch.cuda.empty_cache()
+    # the whole sync of a refined corner
+    nc2 = min(nc, cb.BC_MAX_COMPS)
+    op = cb.Op("hermite", 3, 7)
+    cfab = tiled_fabs((128, 128, 128), (32, 32, 32), (ng,) * 3)
+    ffab = tiled_fabs((128, 128, 128), (32, 32, 32), (ng,) * 3)
+
+    def alloc(fabs):
+        out_ = []
+        for lo, hi, vlo, vhi in fabs:
+            a = torch.full((nc2,) + box_shape(lo, hi), float("nan"), dtype=torch.float64,
+                           device=dev)
+            sl = tuple(slice(vlo[d] - lo[d], vhi[d] - lo[d] + 1) for d in (2, 1, 0))
+            a[(slice(None),) + sl] = torch.rand(a[(slice(None),) + sl].shape, generator=gen,
+                                                dtype=torch.float64, device=dev)
+            out_.append((a, lo, hi, vlo, vhi))
+        return out_
+
+    coarse, finel = alloc(cfab), alloc(ffab)
+    faces = [[(0, 4), (0, 2), (0, 4)], [(0, 2), (0, 4), (0, 2)]]
+    rng = np.random.default_rng(args.seed + 8)
+    cs = boundary_spec(rng, nc2, (1, 1, 1), (128, 128, 128), nghost=ng, faces=faces)
+    fs = boundary_spec(rng, nc2, (1, 1, 1), (256, 256, 256), nghost=ng, faces=faces)
+    fs["dirichlet"], fs["robin"] = cs["dirichlet"], cs["robin"]
+    chain = SyncChain(op, nc2, coarse, finel, (ng,) * 3, cs, fs)
+    cst = chain.stats()
+    chain_bytes = sum(v["bytes"] for v in cst.values())
+    ms_chain = timed_graph(lambda: chain.execute(stream), args.sync_steps)
+    steps_ms = {}
+    for name, p in chain.steps:
+        steps_ms[name] = timed_graph(lambda p=p: p.execute(stream), args.sync_steps)
+    out["sync_chain"] = {
+        "workload": "FillBoundary, coarse-patch gather, coarse boundary conditions, prolongation "
+                    "of the fine patches, scatter, fine boundary conditions: coarse level 128^3 "
+                    "cells in 64 FABs of 32^3, fine level over the lower corner octant in 64 "
+                    f"FABs of 32^3, {ng} ghosts, {nc2} vars, hermite o3 CCC; one CUDA graph",
+        "fine_patches": len(chain.patches), "bytes": chain_bytes, "ms": ms_chain,
+        "achieved_gbs": chain_bytes / (ms_chain / 1e3) / 1e9,
+        "frac_of_peak": chain_bytes / (ms_chain / 1e3) / 1e9 / peak,
+        "steps": {name: {"ms": steps_ms[name], "bytes": cst[name]["bytes"],
+                         "frac_of_peak": cst[name]["bytes"] / (steps_ms[name] / 1e3) / 1e9 / peak}
+                  for name in steps_ms}}
+    chain.close()
     return out
 
 
@@ -861,6 +1002,12 @@ def main():
                 if args.boundary_steps > 0 else None)
     halo = (halo_leg(args, cb, torch, dev, max_over_ranks, barrier, peak)
             if args.halo_steps > 0 else None)
+    sync = None
+    if args.sync_steps > 0:
+        try:
+            sync = sync_leg(args, cb, torch, dev, max_over_ranks, barrier, peak)
+        except Exception as e:  # a failing extra leg does not void the headline line
+            sync = {"error": f"{type(e).__name__}: {e}"}
 
     # per GPU: the ranks' mean algorithmic bytes over the slowest rank's time
     mean_bytes = sum_over_ranks(alg_bytes, dev) / world
@@ -901,6 +1048,7 @@ def main():
         "tuning": tuning,
         "boundary": boundary,
         "halo": halo,
+        "sync": sync,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         lib, kind = cpu_lib()

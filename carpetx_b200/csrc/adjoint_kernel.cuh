@@ -261,7 +261,8 @@ __device__ __forceinline__ void zt_add(double (&acc)[L], double g) {
 // for stencil kinds KX, KY, KZ per direction (buffers sized for the pair).
 // Returns false if a bounded wait gave up (the CTA then stops).
 template <class KV, class KC, class KX, class KY, class KZ>
-__device__ __forceinline__ bool adj_item(double *fbuf, double *gbuf, uint64_t *mbar, int *s_fail,
+__device__ __forceinline__ bool adj_item(long long limit, double *fbuf, double *gbuf, uint64_t *mbar,
+                                         int *s_fail,
                                          uint32_t &phase, const BoxDesc &bd, int xt, int yt, int zt,
                                          int comp) {
   constexpr int FP = AdjPair<KV, KC>::FP, DM = AdjPair<KV, KC>::DM;
@@ -423,7 +424,9 @@ __device__ __forceinline__ bool adj_item(double *fbuf, double *gbuf, uint64_t *m
     cp_async_commit();
     cp_async_wait_dpf();
     const uint32_t par = (phase >> slot) & 1u;
-    if (tid == 0 && !mbar_wait_bounded(mbar + slot, par, g_adj_wait_limit)) {
+    // the limit is read once per kernel; a first poll needs no clock
+    if (tid == 0 && !(limit > 0 && mbar_try(mbar + slot, par)) &&
+        !mbar_wait_bounded(mbar + slot, par, limit)) {
       *s_fail = 1;
       g_adj_timeout = 1;
     }
@@ -513,6 +516,7 @@ __global__ void __launch_bounds__(NT, AdjPair<KV, KC>::OCC)
   }
   __syncthreads();
   uint32_t phase = 0; // completed-phase parity per buffer
+  const long long limit = g_adj_wait_limit;
   // level mode: after item blockIdx.x, a CTA takes the next untaken item of
   // the list (sorted by cost) from the launch's counter (zero before it)
   for (int item = blockIdx.x; item < nitems;) {
@@ -542,7 +546,7 @@ __global__ void __launch_bounds__(NT, AdjPair<KV, KC>::OCC)
     using KY = std::conditional_t<(CM & 2) != 0, KC, KV>;
     using KZ = std::conditional_t<(CM & 1) != 0, KC, KV>;
     const bool ok =
-        adj_item<KV, KC, KX, KY, KZ>(fbuf, gbuf, mbar, &s_fail, phase, *bp, xt, yt, zt, comp);
+        adj_item<KV, KC, KX, KY, KZ>(limit, fbuf, gbuf, mbar, &s_fail, phase, *bp, xt, yt, zt, comp);
     if (!ok)
       break;
     // adj_item ends with a barrier: box_s and s_take may be overwritten

@@ -1,0 +1,128 @@
+"""The ghost-zone sync of a fine level as plans, the order CarpetX's
+FillPatch_ProlongateGhosts runs it (CarpetX/src/fillpatch.cxx:44-137):
+
+  1. FillBoundary of the fine level (same-level halo exchange);
+  2. gather of the coarse patches (ParallelCopy from the coarse level's valid
+     boxes);
+  3. boundary conditions on the coarse patches;
+  4. prolongation of every fine patch from its coarse patch (one level plan);
+  5. scatter of the fine patches into the fine FABs (ParallelCopy, the FABs'
+     valid boxes grown by the ghosts);
+  6. boundary conditions on the fine FABs.
+
+The fine patches of a FAB are its ghost shell minus the valid boxes of the
+level's FABs, as disjoint boxes; each coarse patch is CoarseBox of its fine
+patch.  `SyncChain` builds the six plans once (per regrid) and executes them
+in order on a stream; the executions can be captured in one CUDA graph.
+FABs are CUDA float64 tensors of shape (ncomp, nz, ny, nx) with inclusive
+(lo, hi) boxes and their valid boxes (valid_lo, valid_hi)."""
+import torch
+
+import carpetx_b200 as cb
+
+
+def subtract(a, b):
+    """Box a minus box b as disjoint boxes (inclusive (lo, hi) pairs)."""
+    lo = [max(a[0][d], b[0][d]) for d in range(3)]
+    hi = [min(a[1][d], b[1][d]) for d in range(3)]
+    if any(lo[d] > hi[d] for d in range(3)):
+        return [a]
+    out = []
+    rlo, rhi = list(a[0]), list(a[1])
+    for d in range(3):
+        if rlo[d] < lo[d]:
+            out.append((tuple(rlo), tuple(rhi[:d] + [lo[d] - 1] + rhi[d + 1:])))
+        if rhi[d] > hi[d]:
+            out.append((tuple(rlo[:d] + [hi[d] + 1] + rlo[d + 1:]), tuple(rhi)))
+        rlo[d], rhi[d] = lo[d], hi[d]
+    return out
+
+
+def fine_patches(fabs):
+    """[(fab index, (lo, hi))]: every FAB's box minus the valid boxes of all
+    FABs of the level, as disjoint boxes.  fabs: (lo, hi, valid_lo,
+    valid_hi) per FAB."""
+    out = []
+    for i, (lo, hi, vlo, vhi) in enumerate(fabs):
+        parts = subtract((lo, hi), (vlo, vhi))
+        for j, other in enumerate(fabs):
+            if j != i:
+                parts = [q for p in parts for q in subtract(p, (other[2], other[3]))]
+        out += [(i, p) for p in parts]
+    return out
+
+
+def _shape(lo, hi):
+    return tuple(int(hi[d]) - int(lo[d]) + 1 for d in (2, 1, 0))
+
+
+def _npts(lo, hi):
+    n = 1
+    for s in _shape(lo, hi):
+        n *= s
+    return n
+
+
+class SyncChain:
+    """The six plans of one fine level's ghost sync.  coarse, fine: lists of
+    (tensor, lo, hi, valid_lo, valid_hi); op: the prolongation operator;
+    nghost: the fine FABs' ghost widths; coarse_bc, fine_bc: the groups'
+    boundary-condition specs (cb.bc_struct) on the two levels.  The patch
+    buffers are allocated once here."""
+
+    def __init__(self, op, ncomp, coarse, fine, nghost, coarse_bc, fine_bc):
+        dev = fine[0][0].device
+        self.patches = fine_patches([f[1:] for f in fine])
+        self.cpb = [op.coarse_box(p[0], p[1]) for _, p in self.patches]
+        self.cp = [torch.full((ncomp,) + _shape(lo, hi), float("nan"), dtype=torch.float64,
+                              device=dev) for lo, hi in self.cpb]
+        self.fp = [torch.full((ncomp,) + _shape(p[0], p[1]), float("nan"), dtype=torch.float64,
+                              device=dev) for _, p in self.patches]
+        cpfabs = [(a, lo, hi, lo, hi) for a, (lo, hi) in zip(self.cp, self.cpb)]
+        fpfabs = [(a, p[0], p[1], p[0], p[1]) for a, (_, p) in zip(self.fp, self.patches)]
+        self.prolong_boxes = [
+            dict(op=op, ncomp=ncomp, crse=c, crse_lo=lo, crse_hi=hi, fine=f, fine_lo=p[0],
+                 fine_hi=p[1], reg_lo=p[0], reg_hi=p[1])
+            for c, (lo, hi), f, (_, p) in zip(self.cp, self.cpb, self.fp, self.patches)]
+        self.steps = [
+            ("fill_boundary", cb.CopyPlan.fill_boundary(fine, ncomp, nghost)),
+            ("gather", cb.CopyPlan.parallel_copy(cpfabs, coarse, ncomp)),
+            ("coarse_bc", cb.BoundaryPlan(coarse_bc, [(a, lo, hi) for a, (lo, hi)
+                                                      in zip(self.cp, self.cpb)])),
+            ("prolong", cb.LevelPlan(self.prolong_boxes)),
+            ("scatter", cb.CopyPlan.parallel_copy(fine, fpfabs, ncomp, dst_nghost=nghost)),
+            ("fine_bc", cb.BoundaryPlan(fine_bc, [(f[0], f[1], f[2]) for f in fine])),
+        ]
+
+    def execute(self, stream=None):
+        for _, p in self.steps:
+            p.execute(stream)
+
+    def stats(self):
+        """Per step: algorithmic bytes and launches of one execution."""
+        out = {}
+        for name, p in self.steps:
+            st = p.stats()
+            out[name] = {"bytes": st["bytes"], "launches": st.get("launches")}
+        return out
+
+    def close(self):
+        for _, p in self.steps:
+            p.close()
+
+
+def tiled_fabs(ncells, fab, nghost, origin=(0, 0, 0)):
+    """FAB boxes (lo, hi, valid_lo, valid_hi) tiling the cell-centred block
+    origin .. origin + ncells - 1 with valid boxes of `fab` cells (ncells a
+    multiple of fab per direction), grown by nghost."""
+    out = []
+    nb = [ncells[d] // fab[d] for d in range(3)]
+    for k in range(nb[2]):
+        for j in range(nb[1]):
+            for i in range(nb[0]):
+                t = (i, j, k)
+                vlo = tuple(origin[d] + t[d] * fab[d] for d in range(3))
+                vhi = tuple(vlo[d] + fab[d] - 1 for d in range(3))
+                out.append((tuple(vlo[d] - nghost[d] for d in range(3)),
+                            tuple(vhi[d] + nghost[d] for d in range(3)), vlo, vhi))
+    return out
