@@ -14,6 +14,8 @@ The fine patches of a FAB are its ghost shell minus the valid boxes of the
 level's FABs, as disjoint boxes; each coarse patch is CoarseBox of its fine
 patch.  `SyncChain` builds the six plans once (per regrid) and executes them
 in order on a stream; the executions can be captured in one CUDA graph.
+With fused=True the prolongation writes the fine patches into the fine FABs
+directly and the scatter goes (five plans).
 FABs are CUDA float64 tensors of shape (ncomp, nz, ny, nx) with inclusive
 (lo, hi) boxes and their valid boxes (valid_lo, valid_hi)."""
 import torch
@@ -64,35 +66,53 @@ def _npts(lo, hi):
 
 
 class SyncChain:
-    """The six plans of one fine level's ghost sync.  coarse, fine: lists of
+    """The plans of one fine level's ghost sync.  coarse, fine: lists of
     (tensor, lo, hi, valid_lo, valid_hi); op: the prolongation operator;
     nghost: the fine FABs' ghost widths; coarse_bc, fine_bc: the groups'
     boundary-condition specs (cb.bc_struct) on the two levels.  The patch
-    buffers are allocated once here."""
+    buffers are allocated once here.
 
-    def __init__(self, op, ncomp, coarse, fine, nghost, coarse_bc, fine_bc):
+    fused=True merges steps 4 and 5: every fine patch lies in its own FAB's
+    ghost region, so the prolongation writes it there directly, and the fine
+    patch buffers and the scatter go.  The result is the same bit for bit:
+    the scatter writes each ghost point not covered by a valid box from a
+    patch of the same position, and a prolongated value depends only on its
+    position and the coarse patch data, which every patch holds alike."""
+
+    def __init__(self, op, ncomp, coarse, fine, nghost, coarse_bc, fine_bc, fused=False):
         dev = fine[0][0].device
+        self.fused = fused
         self.patches = fine_patches([f[1:] for f in fine])
         self.cpb = [op.coarse_box(p[0], p[1]) for _, p in self.patches]
         self.cp = [torch.full((ncomp,) + _shape(lo, hi), float("nan"), dtype=torch.float64,
                               device=dev) for lo, hi in self.cpb]
-        self.fp = [torch.full((ncomp,) + _shape(p[0], p[1]), float("nan"), dtype=torch.float64,
-                              device=dev) for _, p in self.patches]
         cpfabs = [(a, lo, hi, lo, hi) for a, (lo, hi) in zip(self.cp, self.cpb)]
-        fpfabs = [(a, p[0], p[1], p[0], p[1]) for a, (_, p) in zip(self.fp, self.patches)]
-        self.prolong_boxes = [
-            dict(op=op, ncomp=ncomp, crse=c, crse_lo=lo, crse_hi=hi, fine=f, fine_lo=p[0],
-                 fine_hi=p[1], reg_lo=p[0], reg_hi=p[1])
-            for c, (lo, hi), f, (_, p) in zip(self.cp, self.cpb, self.fp, self.patches)]
+        if fused:
+            self.fp = []
+            self.prolong_boxes = [
+                dict(op=op, ncomp=ncomp, crse=c, crse_lo=lo, crse_hi=hi, fine=fine[i][0],
+                     fine_lo=fine[i][1], fine_hi=fine[i][2], reg_lo=p[0], reg_hi=p[1])
+                for c, (lo, hi), (i, p) in zip(self.cp, self.cpb, self.patches)]
+        else:
+            self.fp = [torch.full((ncomp,) + _shape(p[0], p[1]), float("nan"),
+                                  dtype=torch.float64, device=dev) for _, p in self.patches]
+            self.prolong_boxes = [
+                dict(op=op, ncomp=ncomp, crse=c, crse_lo=lo, crse_hi=hi, fine=f, fine_lo=p[0],
+                     fine_hi=p[1], reg_lo=p[0], reg_hi=p[1])
+                for c, (lo, hi), f, (_, p) in zip(self.cp, self.cpb, self.fp, self.patches)]
         self.steps = [
             ("fill_boundary", cb.CopyPlan.fill_boundary(fine, ncomp, nghost)),
             ("gather", cb.CopyPlan.parallel_copy(cpfabs, coarse, ncomp)),
             ("coarse_bc", cb.BoundaryPlan(coarse_bc, [(a, lo, hi) for a, (lo, hi)
                                                       in zip(self.cp, self.cpb)])),
             ("prolong", cb.LevelPlan(self.prolong_boxes)),
-            ("scatter", cb.CopyPlan.parallel_copy(fine, fpfabs, ncomp, dst_nghost=nghost)),
-            ("fine_bc", cb.BoundaryPlan(fine_bc, [(f[0], f[1], f[2]) for f in fine])),
         ]
+        if not fused:
+            fpfabs = [(a, p[0], p[1], p[0], p[1]) for a, (_, p) in zip(self.fp, self.patches)]
+            self.steps.append(("scatter", cb.CopyPlan.parallel_copy(fine, fpfabs, ncomp,
+                                                                     dst_nghost=nghost)))
+        self.steps.append(("fine_bc", cb.BoundaryPlan(fine_bc, [(f[0], f[1], f[2])
+                                                                for f in fine])))
 
     def execute(self, stream=None):
         for _, p in self.steps:
