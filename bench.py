@@ -546,6 +546,31 @@ def sync_leg(args, cb, torch, dev, max_over_ranks, barrier, peak):
                   "frac_of_peak": fused_bytes / (ms_fused / 1e3) / 1e9 / peak,
                   "speedup": ms_chain / ms_fused}}
     chain.close()
+    # reflux of the refined corner's coarse level (CarpetX's Reflux through
+    # the FluxRegister): face-centred fluxes on both levels, the same FABs
+    def flux_fabs(fabs, d):
+        out_ = []
+        for a, lo, hi, vlo, vhi in fabs:
+            flo, fhi = lo, tuple(v + (e == d) for e, v in enumerate(hi))
+            fvhi = tuple(v + (e == d) for e, v in enumerate(vhi))
+            t = torch.empty((nc2,) + box_shape(flo, fhi), dtype=torch.float64, device=dev)
+            t.normal_(generator=gen)
+            out_.append((t, flo, fhi, vlo, fvhi))
+        return out_
+
+    cfx = [flux_fabs(coarse, d) for d in range(3)]
+    ffx = [flux_fabs(finel, d) for d in range(3)]
+    rplan = cb.RefluxPlan(coarse, cfx, ffx, nc2, (1.0 / 128,) * 3)
+    rst = rplan.stats()
+    ms_r = timed_graph(lambda: rplan.execute(stream), args.sync_steps)
+    out["reflux"] = {
+        "workload": "the coarse level of the refined corner above: every face of the fine "
+                    f"boxes' coarsened boundary with a coarse cell outside, {nc2} vars; "
+                    "CrseInit, FineAdd and Reflux fused, one launch per face orientation",
+        "faces": rst["faces"], "bytes": rst["bytes"], "launches": rst["launches"], "ms": ms_r,
+        "faces_per_s": rst["faces"] * nc2 / (ms_r / 1e3),
+        "frac_of_peak": rst["bytes"] / (ms_r / 1e3) / 1e9 / peak}
+    rplan.close()
     return out
 
 

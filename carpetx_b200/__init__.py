@@ -163,6 +163,15 @@ def lib():
                                          ctypes.POINTER(ctypes.c_int64),
                                          ctypes.POINTER(ctypes.c_int64)]
         L.cx_copy_plan_destroy.argtypes = [_VP]
+        L.cx_reflux_plan_create.argtypes = [ctypes.POINTER(CxFab), _I,
+                                            ctypes.POINTER(ctypes.POINTER(CxFab)),
+                                            ctypes.POINTER(ctypes.POINTER(CxFab)), _I, _I,
+                                            ctypes.POINTER(ctypes.c_double), ctypes.c_double,
+                                            ctypes.POINTER(_VP)]
+        L.cx_reflux_plan_execute.argtypes = [_VP, _VP]
+        L.cx_reflux_plan_stats.argtypes = [_VP, ctypes.POINTER(ctypes.c_int64),
+                                           ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(_I)]
+        L.cx_reflux_plan_destroy.argtypes = [_VP]
         L.cx_restrict_plan_create.argtypes = [ctypes.POINTER(CxRestrictBox), _I,
                                               ctypes.POINTER(_VP)]
         L.cx_restrict_plan_execute.argtypes = [_VP, _VP]
@@ -508,6 +517,56 @@ class LevelPlan:
     def close(self):
         if self.handle:
             lib().cx_level_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RefluxPlan:
+    """cx_reflux_plan_*: the reflux of a coarse level from the next finer
+    one (CarpetX's Reflux(), AMReX FluxRegister semantics).  crse: the
+    coarse state FABs; crse_flux[d]: per direction the coarse flux FABs (one
+    per state FAB); fine_flux[d]: per direction the fine flux FABs (one per
+    fine box); each FAB a tuple (tensor, lo, hi, valid_lo, valid_hi) as for
+    CopyPlan.  dx: the coarse cell size; the plan keeps the tensors alive."""
+
+    def __init__(self, crse, crse_flux, fine_flux, ncomp, dx, scale=1.0):
+        self._keep = []
+        arr_c = CopyPlan._fabs(list(crse), ncomp)
+        self._keep.append(arr_c)
+        cf = (ctypes.POINTER(CxFab) * 3)()
+        ff = (ctypes.POINTER(CxFab) * 3)()
+        nfine = len(fine_flux[0])
+        for d in range(3):
+            a = CopyPlan._fabs(list(crse_flux[d]), ncomp)
+            b = CopyPlan._fabs(list(fine_flux[d]), ncomp)
+            self._keep += [a, b]
+            cf[d] = ctypes.cast(a, ctypes.POINTER(CxFab))
+            ff[d] = ctypes.cast(b, ctypes.POINTER(CxFab))
+        self._keep += [f[0] for f in crse] + [f[0] for d in range(3) for f in crse_flux[d]]
+        self._keep += [f[0] for d in range(3) for f in fine_flux[d]]
+        h = ctypes.c_void_p()
+        _check(lib().cx_reflux_plan_create(arr_c, len(crse), cf, ff, nfine, int(ncomp),
+                                           (ctypes.c_double * 3)(*dx), float(scale),
+                                           ctypes.byref(h)))
+        self.handle = h
+
+    def execute(self, stream=None):
+        _check(lib().cx_reflux_plan_execute(self.handle, _stream(stream)))
+
+    def stats(self):
+        a, b, n = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int()
+        _check(lib().cx_reflux_plan_stats(self.handle, ctypes.byref(a), ctypes.byref(b),
+                                          ctypes.byref(n)))
+        return {"faces": a.value, "bytes": b.value, "launches": n.value}
+
+    def close(self):
+        if self.handle:
+            lib().cx_reflux_plan_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -404,6 +404,37 @@ typedef struct {
 
 typedef struct cx_copy_plan *cx_copy_plan_t;
 
+/* Reflux of one coarse level from the next finer (Reflux(),
+ * CarpetX/src/schedule.cxx:2632-2713), replacing AMReX's FluxRegister
+ * (built at driver.cxx:918-924; AMReX 25.11 is not in the reference tree):
+ * per direction d CrseInit(coarse flux_d, d, 0, 0, ncomp, -1) and
+ * FineAdd(fine flux_d, d, 0, 0, ncomp, +1), then Reflux(coarse state,
+ * scale, 0, 0, ncomp, coarse geometry).  For every face of a fine box's
+ * coarsened boundary, reg = -(coarse flux) + the fine fluxes of the 2 x 2
+ * fine faces covering it (the higher transverse direction outer), and the
+ * coarse cell just outside the fine box gets -scale * reg / vol across a low
+ * face and +scale * reg / vol across a high face (vol = dx[0] dx[1] dx[2]),
+ * orientation by orientation: x, y, z low, then x, y, z high.  The coarse
+ * flux of a face comes from the first coarse flux FAB whose valid faces hold
+ * it.  Coarse cells under other fine boxes are corrected too, as in AMReX;
+ * the restriction that follows overwrites them.
+ *   crse: the coarse state FABs (cell centred); crse_flux[d]: per direction
+ *   the coarse flux FABs (ncrse each, same order, valid box = the state's
+ *   face centred in d); fine_flux[d]: per direction the fine flux FABs, one
+ *   per fine box (valid box = the box's cells face centred in d; the boxes
+ *   must be coarsenable by 2).  The plan holds a device list of the faces;
+ *   executing it launches once per orientation that has faces. */
+typedef struct cx_reflux_plan *cx_reflux_plan_t;
+int cx_reflux_plan_create(const cx_fab_t *crse, int ncrse, const cx_fab_t *const crse_flux[3],
+                          const cx_fab_t *const fine_flux[3], int nfine, int ncomp,
+                          const double dx[3], double scale, cx_reflux_plan_t *out);
+int cx_reflux_plan_execute(cx_reflux_plan_t plan, cx_stream_t stream);
+/* Register faces per execution (coarse faces x orientations), algorithmic
+ * bytes (per face and component: the coarse flux, four fine fluxes, the
+ * coarse value read and written) and launches per execution. */
+int cx_reflux_plan_stats(cx_reflux_plan_t plan, int64_t *faces, int64_t *bytes, int *launches);
+int cx_reflux_plan_destroy(cx_reflux_plan_t plan);
+
 /* dst.ParallelCopy(src, 0, 0, ncomp, src_nghost, dst_nghost, period): every
  * point of each destination FAB's valid box grown by dst_nghost (clipped to
  * the FAB) is set from the first source FAB whose valid box grown by
