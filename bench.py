@@ -395,6 +395,23 @@ def limited_leg(args, cb, torch, dev, max_over_ranks, barrier):
         out[f"{typ}_pts_per_s"] = out["fine_points"] / (ms / 1e3)
         out[f"{typ}_launches"] = plan.stats()["launches"]
         plan.close()
+        if not untuned:
+            # the adjoint level plan, linearised at the same coarse data
+            # (decision pass and gather per box): P^T of the fine data
+            cbar = [torch.empty_like(c) for c in crse]
+            aplan = cb.LevelPlan([dict(b, crse=cb_, crse_at=b["crse"])
+                                  for b, cb_ in zip(boxes, cbar)], adjoint=True)
+            aplan.execute()
+            barrier()
+            e0.record()
+            aplan.execute()
+            e1.record()
+            barrier()
+            ms_a = max_over_ranks(e0.elapsed_time(e1))
+            out[f"{typ}_adjoint_ms"] = ms_a
+            out[f"{typ}_adjoint_over_forward"] = ms_a / ms
+            aplan.close()
+            del cbar
         del boxes
     return out
 

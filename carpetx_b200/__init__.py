@@ -137,6 +137,8 @@ def lib():
         L.cx_level_plan_create.argtypes = [ctypes.POINTER(CxBox), _I, _I, ctypes.POINTER(_VP)]
         L.cx_level_plan_create_adjoint.argtypes = [ctypes.POINTER(CxBox), _I, _I,
                                                    ctypes.POINTER(_VP)]
+        L.cx_level_plan_create_adjoint_at.argtypes = [ctypes.POINTER(CxBox), ctypes.POINTER(_VP),
+                                                      _I, _I, ctypes.POINTER(_VP)]
         L.cx_level_plan_execute.argtypes = [_VP, _VP]
         L.cx_level_plan_stats.argtypes = [_VP, ctypes.POINTER(ctypes.c_int64),
                                           ctypes.POINTER(ctypes.c_int64),
@@ -484,7 +486,10 @@ class LevelPlan:
     fine_lo, fine_hi, reg_lo, reg_hi (tensors as for prolong_box).  The plan
     keeps references to the tensors so their memory outlives it.  With
     adjoint=True (cx_level_plan_create_adjoint) executing the plan overwrites
-    every crse tensor with P^T of its fine tensor (region points only)."""
+    every crse tensor with P^T of its fine tensor (region points only); a
+    box of a limited operator (ENO, minmod, linear fallback) also carries
+    crse_at, the coarse data it is linearised at
+    (cx_level_plan_create_adjoint_at)."""
 
     def __init__(self, boxes, per_group=False, adjoint=False):
         self._keep = []
@@ -499,8 +504,19 @@ class LevelPlan:
                            _i3(b["reg_hi"]))
             self._keep += [b["crse"], b["fine"]]
         h = ctypes.c_void_p()
-        create = lib().cx_level_plan_create_adjoint if adjoint else lib().cx_level_plan_create
-        _check(create(arr, len(boxes), int(bool(per_group)), ctypes.byref(h)))
+        if adjoint and any(b.get("crse_at") is not None for b in boxes):
+            # the limited operators' linearisation points (cx_level_plan_create_adjoint_at)
+            at = (_VP * max(1, len(boxes)))()
+            for i, b in enumerate(boxes):
+                if b.get("crse_at") is not None:
+                    n = int(b["ncomp"])
+                    at[i] = _ptr(b["crse_at"], n, b["crse_lo"], b["crse_hi"], "crse_at").value
+                    self._keep.append(b["crse_at"])
+            _check(lib().cx_level_plan_create_adjoint_at(arr, at, len(boxes), int(bool(per_group)),
+                                                         ctypes.byref(h)))
+        else:
+            create = lib().cx_level_plan_create_adjoint if adjoint else lib().cx_level_plan_create
+            _check(create(arr, len(boxes), int(bool(per_group)), ctypes.byref(h)))
         self.handle = h
 
     def execute(self, stream=None):

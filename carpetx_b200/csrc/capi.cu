@@ -200,6 +200,10 @@ struct cx_level_plan {
   // boxes whose region is empty are zeroed (pointer, bytes)
   bool adjoint = false;
   std::vector<std::pair<double *, size_t>> zero_boxes;
+  // adjoint plan: scratch of the limited operators' decision passes (the
+  // point boxes run one after the other on the stream, so one buffer of the
+  // largest box's size serves them all)
+  void *d_scratch = nullptr;
 };
 
 extern "C" {
@@ -412,6 +416,11 @@ int cx_level_plan_create(const cx_box_t *boxes, int nboxes, int per_group, cx_le
 
 int cx_level_plan_create_adjoint(const cx_box_t *boxes, int nboxes, int per_group,
                                  cx_level_plan_t *out) {
+  return cx_level_plan_create_adjoint_at(boxes, nullptr, nboxes, per_group, out);
+}
+
+int cx_level_plan_create_adjoint_at(const cx_box_t *boxes, const double *const *crse_at,
+                                    int nboxes, int per_group, cx_level_plan_t *out) {
   if (!out || nboxes < 0 || (nboxes > 0 && !boxes))
     return fail(CX_EINVAL, "invalid argument");
   *out = nullptr;
@@ -421,6 +430,7 @@ int cx_level_plan_create_adjoint(const cx_box_t *boxes, int nboxes, int per_grou
   p->per_group = per_group;
   p->adjoint = true;
   std::vector<int> ids;
+  size_t scratch = 0;
   for (int i = 0; i < nboxes; ++i) {
     const cx_box_t &x = boxes[i];
     BoxDesc b;
@@ -440,12 +450,27 @@ int cx_level_plan_create_adjoint(const cx_box_t *boxes, int nboxes, int per_grou
                                  sizeof(double) * box_points(x.crse_lo, x.crse_hi) * x.ncomp});
       continue;
     }
-    if (!op_separable(x.op, per_group) || adjoint_pair_of(b) < 0) {
-      delete p;
-      return fail(CX_EUNSUPPORTED, "box %d: adjoint of limited operators (ENO, minmod, linear "
-                                   "fallback) is not available", i);
-    }
     b.cbar = const_cast<double *>(x.crse);
+    if (!op_separable(x.op, per_group) || adjoint_pair_of(b) < 0) {
+      // limited operators (ENO, minmod, active linear fallback): a decision
+      // pass and a gather per box, after the streaming groups, linearised at
+      // the box's coarse data crse_at[i] (crse is the output)
+      if (!crse_at || !crse_at[i]) {
+        cx_level_plan_destroy(p);
+        return fail(CX_EINVAL, "box %d: the adjoint of a limited operator (ENO, minmod, linear "
+                               "fallback) needs the coarse data it is linearised at "
+                               "(cx_level_plan_create_adjoint_at)", i);
+      }
+      b.crse = crse_at[i];
+      int cl[3], ch[3];
+      cx_prolong_coarse_box(x.op, x.reg_lo, x.reg_hi, cl, ch);
+      p->nfine += box_points(x.reg_lo, x.reg_hi) * x.ncomp;
+      p->bytes += 8 * (box_points(cl, ch) + box_points(x.reg_lo, x.reg_hi)) * x.ncomp;
+      scratch = std::max(scratch, point_adjoint_scratch_bytes(b, per_group));
+      p->point_boxes.push_back((int)p->boxes.size());
+      p->boxes.push_back(b);
+      continue;
+    }
     adjoint_tiling(b, 0);
     if (b.ant[0] > INT16_MAX || b.ant[1] > INT16_MAX || b.ant[2] > INT16_MAX ||
         x.ncomp > INT16_MAX) {
@@ -512,6 +537,8 @@ int cx_level_plan_create_adjoint(const cx_box_t *boxes, int nboxes, int per_grou
   if (e == cudaSuccess && !tiles.empty())
     e = cudaMemcpy(p->d_tiles, tiles.data(), sizeof(TileRef) * tiles.size(),
                    cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && scratch)
+    e = cudaMalloc(&p->d_scratch, scratch);
   if (e != cudaSuccess) {
     cx_level_plan_destroy(p);
     return fail(e == cudaErrorMemoryAllocation ? CX_ENOMEM : CX_ECUDA, "level plan: %s",
@@ -547,6 +574,12 @@ int cx_level_plan_execute(cx_level_plan_t p, cx_stream_t stream) {
         after_level = true;
       }
     }
+    // the limited operators' boxes: a decision pass and a gather each
+    for (int id : p->point_boxes)
+      if (int e = cuda_status(launch_point_adjoint_box_scratch(p->boxes[id], p->per_group,
+                                                               p->boxes[id].cbar, p->d_scratch, s),
+                              "adjoint launch (limited operators)"))
+        return e;
     return CX_OK;
   }
   if (p->d_counters)
@@ -637,6 +670,9 @@ int cx_level_plan_launches(cx_level_plan_t p, int *nlaunches) {
     n += p->group_off[g + 1] > p->group_off[g];
   if (!p->adjoint)
     n += (int)p->point_boxes.size();
+  else
+    for (int id : p->point_boxes) // decision pass (if any) and gather
+      n += 1 + (point_adjoint_scratch_bytes(p->boxes[id], p->per_group) > 0);
   *nlaunches = n;
   return CX_OK;
 }
@@ -647,6 +683,7 @@ int cx_level_plan_destroy(cx_level_plan_t p) {
   cudaFree(p->d_boxes);
   cudaFree(p->d_tiles);
   cudaFree(p->d_counters);
+  cudaFree(p->d_scratch);
   delete p;
   return CX_OK;
 }

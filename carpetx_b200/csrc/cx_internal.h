@@ -145,6 +145,11 @@ cudaError_t launch_prolong_adjoint_box(const BoxDesc &b, int per_group,
 // decision pass into stream-ordered scratch, then a gather per coarse point.
 cudaError_t launch_point_adjoint_box(const BoxDesc &b, int per_group,
                                      double *crse_bar, cudaStream_t s);
+// The same with the caller's scratch of at least
+// point_adjoint_scratch_bytes(b, per_group) bytes (0: none needed).
+size_t point_adjoint_scratch_bytes(const BoxDesc &b, int per_group);
+cudaError_t launch_point_adjoint_box_scratch(const BoxDesc &b, int per_group, double *crse_bar,
+                                             void *scratch, cudaStream_t s);
 // Adjoint tiling of a box (cbar must be set by the caller); min_items > 0
 // shortens the z chunks of a box launched alone so that it spreads over at
 // least that many CTAs where it can.

@@ -442,29 +442,37 @@ cudaError_t launch_point_box(const BoxDesc &b, int per_group, signed char *shift
   return cudaGetLastError();
 }
 
-// Adjoint of a limited operator on one box: decision pass into stream-ordered
-// scratch (the ENO shift and fallback flag of every region point, recomputed
-// from crse), then the gather.  fine in b holds fine_bar.
-cudaError_t launch_point_adjoint_box(const BoxDesc &b, int per_group, double *crse_bar,
-                                     cudaStream_t s) {
-  if (b.ncomp <= 0 || b.cnp <= 0)
-    return cudaSuccess;
+// Scratch the adjoint of a limited operator needs on one box: the ENO shift
+// (3 bytes) and fallback flag (1 byte) of every region point and component
+// block, when it has ENO directions or an active linear fallback; else 0.
+size_t point_adjoint_scratch_bytes(const BoxDesc &b, int per_group) {
   const int64_t rnp = (int64_t)(b.rhi[0] - b.rlo[0] + 1) * (b.rhi[1] - b.rlo[1] + 1) *
                       (b.rhi[2] - b.rlo[2] + 1);
-  const int nblk = per_group ? 1 : b.ncomp;
   bool eno = false;
   for (int d = 0; d < 3; ++d)
     eno = eno || b.kind[d] == K_CC_ENO2;
-  const bool decide = eno || op_fb_active(b.op, per_group);
+  if (b.ncomp <= 0 || rnp <= 0 || !(eno || op_fb_active(b.op, per_group)))
+    return 0;
+  return (size_t)4 * rnp * (per_group ? 1 : b.ncomp);
+}
+
+// Adjoint of a limited operator on one box with the caller's scratch (at
+// least point_adjoint_scratch_bytes): decision pass (the ENO shift and
+// fallback flag of every region point, recomputed from crse), then the
+// gather.  fine in b holds fine_bar.
+cudaError_t launch_point_adjoint_box_scratch(const BoxDesc &b, int per_group, double *crse_bar,
+                                             void *scratch, cudaStream_t s) {
+  if (b.ncomp <= 0 || b.cnp <= 0)
+    return cudaSuccess;
+  const int nblk = per_group ? 1 : b.ncomp;
+  const size_t need = point_adjoint_scratch_bytes(b, per_group);
   signed char *sh = nullptr;
   unsigned char *fb = nullptr;
-  void *scratch = nullptr;
   cudaError_t e = cudaSuccess;
-  if (decide && rnp > 0) {
-    const size_t n = (size_t)rnp * nblk;
-    e = cudaMallocAsync(&scratch, 4 * n, s);
-    if (e != cudaSuccess)
-      return e;
+  if (need) {
+    if (!scratch)
+      return cudaErrorInvalidValue;
+    const size_t n = need / 4;
     sh = static_cast<signed char *>(scratch);
     fb = reinterpret_cast<unsigned char *>(sh + 3 * n);
     BoxDesc d = b;
@@ -473,14 +481,27 @@ cudaError_t launch_point_adjoint_box(const BoxDesc &b, int per_group, double *cr
   }
   if (e == cudaSuccess) {
     const int64_t nb = (b.cnp + AT_NT - 1) / AT_NT;
-    if (nb > INT32_MAX) {
-      e = cudaErrorInvalidValue;
-    } else {
-      adjoint_point_kernel<<<dim3((unsigned)nb, nblk), AT_NT, 0, s>>>(b, per_group, sh, fb,
-                                                                       crse_bar);
-      e = cudaGetLastError();
-    }
+    if (nb > INT32_MAX)
+      return cudaErrorInvalidValue;
+    adjoint_point_kernel<<<dim3((unsigned)nb, nblk), AT_NT, 0, s>>>(b, per_group, sh, fb,
+                                                                     crse_bar);
+    e = cudaGetLastError();
   }
+  return e;
+}
+
+// The same for one box with stream-ordered scratch (cudaMallocAsync /
+// cudaFreeAsync around the launches).
+cudaError_t launch_point_adjoint_box(const BoxDesc &b, int per_group, double *crse_bar,
+                                     cudaStream_t s) {
+  const size_t need = point_adjoint_scratch_bytes(b, per_group);
+  void *scratch = nullptr;
+  if (need) {
+    const cudaError_t e = cudaMallocAsync(&scratch, need, s);
+    if (e != cudaSuccess)
+      return e;
+  }
+  cudaError_t e = launch_point_adjoint_box_scratch(b, per_group, crse_bar, scratch, s);
   if (scratch) {
     const cudaError_t e2 = cudaFreeAsync(scratch, s);
     if (e == cudaSuccess)

@@ -180,11 +180,22 @@ int cx_level_plan_destroy(cx_level_plan_t plan);
  * array (whole coarse box, every component) with P^T of its fine array,
  * reading the fine array only inside the region, as cx_prolong_adjoint_box
  * does box by box; one persistent launch per stencil pair and centring
- * present.  Validation is cx_prolong_box's; operators without a linear
- * separable form (ENO, minmod, active linear fallback) give
- * CX_EUNSUPPORTED.  Executed, destroyed and queried like any level plan. */
+ * present.  Validation is cx_prolong_box's.  Executed, destroyed and queried
+ * like any level plan.  The limited operators (ENO, minmod, active linear
+ * fallback) need cx_level_plan_create_adjoint_at: here they give
+ * CX_EINVAL. */
 int cx_level_plan_create_adjoint(const cx_box_t *boxes, int nboxes,
                                  int per_group, cx_level_plan_t *out);
+/* The same with the coarse data the limited operators are linearised at:
+ * crse_at[i] holds box i's coarse input (the layout of its crse array; may
+ * be null for linear operators).  As cx_prolong_adjoint_box, P^T is taken
+ * with each fine point's choices (ENO shift, minmod branch, linear fallback)
+ * recomputed from crse_at: after the streaming launches, every box of a
+ * limited operator takes a decision pass into scratch the plan allocates
+ * once, then a gather.  Executions of one plan must not overlap (the
+ * scratch is the plan's). */
+int cx_level_plan_create_adjoint_at(const cx_box_t *boxes, const double *const *crse_at,
+                                    int nboxes, int per_group, cx_level_plan_t *out);
 
 /* ---------------------------------------------------------------------- */
 /* A whole level without allocating device memory                          */

@@ -335,9 +335,59 @@ def test_gpu_adjoint_level_plan(dev, cx):
     lim["crse_lo"], lim["crse_hi"] = cx.coarse_box("minmod", 3, 7, lim["fine_lo"], lim["fine_hi"])
     lim["crse"] = torch.zeros((2,) + box_shape(lim["crse_lo"], lim["crse_hi"]),
                               dtype=torch.float64, device="cuda")
+    # a limited operator needs the coarse data it is linearised at
     with pytest.raises(cb.CxError) as e:
         cb.LevelPlan([lim], adjoint=True)
-    assert e.value.status == cb.CX_EUNSUPPORTED
+    assert e.value.status == cb.CX_EINVAL
+
+
+@pytest.mark.parametrize("pg", [0, 1])
+def test_gpu_adjoint_level_plan_limited(dev, cx, pg):
+    """cx_level_plan_create_adjoint_at: a level mixing limited operators (ENO,
+    minmod, active linear fallback, linearised at each box's coarse input)
+    with linear ones; every box's coarse array equals cx_prolong_adjoint_box
+    bit for bit and the oracle's transpose within roundoff, over two
+    executions (the plan's decision scratch is reused)."""
+    from helpers import random_case
+    rng = np.random.default_rng(21 + pg)
+    specs = [("eno", 3, 7), ("minmod", 1, 7), ("interpolate", 5, 0), ("poly-cons3lfb", 3, 7),
+             ("eno", 5, 1), ("minmod", 3, 3), ("hermite", 3, 3), ("poly-eno3lfb", 5, 6)]
+    boxes = []
+    for i, (typ, order, it) in enumerate(specs):
+        c = random_case(rng, cx, typ, order, it, ncomp=3, max_n=24,
+                        kind="jumps" if i % 2 else "normal")
+        v = rng.standard_normal((3,) + box_shape(c["flo"], c["fhi"]))
+        boxes.append(dict(op=cb.Op(typ, order, it), typ=typ, order=order, it=it, ncomp=3,
+                          crse=torch.full(c["crse"].shape, np.nan, dtype=torch.float64,
+                                          device="cuda"),
+                          crse_at=cuda(c["crse"]), u=c["crse"], crse_lo=c["clo"],
+                          crse_hi=c["chi"], fine=cuda(v), fine_np=v, fine_lo=c["flo"],
+                          fine_hi=c["fhi"], reg_lo=c["rlo"], reg_hi=c["rhi"]))
+    plan = cb.LevelPlan([{k: b[k] for k in ("op", "ncomp", "crse", "crse_at", "crse_lo",
+                                            "crse_hi", "fine", "fine_lo", "fine_hi", "reg_lo",
+                                            "reg_hi")} for b in boxes], per_group=bool(pg),
+                        adjoint=True)
+    for _ in range(2):
+        plan.execute()
+    torch.cuda.synchronize()
+    assert cb.lib().cx_check_device() == cb.CX_OK
+    for i, b in enumerate(boxes):
+        got = b["crse"].cpu().numpy()
+        one = torch.full_like(b["crse"], np.nan)
+        cb.prolong_adjoint_box(b["op"], b["crse_at"], b["crse_lo"], b["crse_hi"], b["fine"],
+                               b["fine_lo"], b["fine_hi"], b["reg_lo"], b["reg_hi"], 3, one,
+                               per_group=bool(pg))
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(got, one.cpu().numpy(), err_msg=f"box {i} {b['typ']}")
+        mask = region_mask(b["fine_lo"], b["fine_hi"], b["reg_lo"], b["reg_hi"])
+        want = np.zeros_like(got)
+        cx.prolong_adjoint(b["typ"], b["order"], b["it"], pg, b["u"], b["crse_lo"], b["crse_hi"],
+                           b["fine_np"] * mask, b["fine_lo"], b["fine_hi"], b["reg_lo"],
+                           b["reg_hi"], 3, want)
+        scale = max(1.0, np.abs(want).max())
+        np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12 * scale,
+                                   err_msg=f"box {i} {b['typ']} o{b['order']} it{b['it']}")
+    plan.close()
 
 
 @pytest.mark.parametrize("typ,order,it", [("eno", 3, 7), ("eno", 5, 1), ("minmod", 1, 7),
