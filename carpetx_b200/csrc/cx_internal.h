@@ -113,9 +113,16 @@ cudaError_t launch_point_box(const BoxDesc &b, int per_group,
 // The per-coarse-cell ENO kernel takes operators whose three directions are
 // CC ENO 2 without an active linear fallback (launch_point_box forwards).
 bool eno_cell_applies(const BoxDesc &b, int per_group);
+// cshift: decisions only, one shift code per coarse cell (the adjoint's).
 cudaError_t launch_eno_cell_box(const BoxDesc &b, int per_group, signed char *shifts,
                                 unsigned char *fallback, cudaStream_t s,
-                                bool after_level = false);
+                                bool after_level = false, unsigned char *cshift = nullptr);
+// Adjoint of the ENO-per-cell operators on one box: the decision pass into
+// scratch (eno_adjoint_scratch_bytes: one byte per coarse cell with
+// children in the region and component block), then a tiled gather.
+size_t eno_adjoint_scratch_bytes(const BoxDesc &b, int per_group);
+cudaError_t launch_eno_adjoint_box(const BoxDesc &b, int per_group, void *scratch,
+                                   double *crse_bar, cudaStream_t s);
 cudaError_t launch_point_level(const BoxDesc *d_boxes, const TileRef *d_tiles,
                                int ntiles, int per_group, cudaStream_t s);
 

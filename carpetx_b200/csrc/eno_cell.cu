@@ -75,13 +75,19 @@ __device__ __forceinline__ double eno2_apply(const double w[3], double t0, doubl
 
 struct EnoTiling {
   int clo[3];   // first coarse cell of the region (rlo >> 1)
+  int nc[3];    // coarse cells with children in the region, per direction
   int nt[3];    // tiles per direction
   int nblk;     // component blocks: ncomp (per var) or 1 (per group)
 };
 
+// cshift (decisions for the adjoint, or null): the chosen shift of every
+// coarse cell with children in the region, per component block, one byte
+// (sx + 1) + 3 (sy + 1) + 9 (sz + 1), cells x fastest over t.nc; with it the
+// children are not evaluated.
+template <bool DECIDE>
 __global__ void __launch_bounds__(ENT, 2)
     eno_cell_kernel(const __grid_constant__ BoxDesc b, const EnoTiling t, int per_group,
-                    signed char *shifts, unsigned char *fallback) {
+                    signed char *shifts, unsigned char *fallback, unsigned char *cshift) {
   // the launches of a level's boxes after its first start in the previous
   // launch's tail and wait for it at their end (programmatic dependent
   // launch; no-ops without the launch attribute)
@@ -242,6 +248,26 @@ __global__ void __launch_bounds__(ENT, 2)
       shx[q] = best % 3 - 1;
       shy[q] = (best / 3) % 3 - 1;
       shz[q] = best / 9 - 1;
+      if constexpr (DECIDE) {
+        const int lx = o0 + 2 + ci - t.clo[0], ly = o1 + 2 + cj - t.clo[1],
+                  lz = o2 + 2 + ck - t.clo[2];
+        if (lx < t.nc[0] && ly < t.nc[1] && lz < t.nc[2])
+          cshift[(int64_t)blk * t.nc[0] * t.nc[1] * t.nc[2] + lx +
+                 (int64_t)t.nc[0] * (ly + (int64_t)t.nc[1] * lz)] = (unsigned char)best;
+      }
+    }
+    if constexpr (DECIDE) { // decisions only: no children to evaluate
+      if (item + (int)gridDim.x < nitems) {
+        int p0, p1, p2, pblk;
+        origin(item + gridDim.x, p0, p1, p2, pblk);
+        load(Cn, p0, p1, p2, per_group ? 0 : pblk, true);
+      }
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
+      __syncthreads();
+      double *const t_ = Cc;
+      Cc = Cn;
+      Cn = t_;
+      continue;
     }
 
     // copy the first window of this CTA's next item into the other buffer
@@ -349,7 +375,8 @@ bool eno_cell_applies(const BoxDesc &b, int per_group) {
 }
 
 cudaError_t launch_eno_cell_box(const BoxDesc &b, int per_group, signed char *shifts,
-                                unsigned char *fallback, cudaStream_t s, bool after_level) {
+                                unsigned char *fallback, cudaStream_t s, bool after_level,
+                                unsigned char *cshift) {
   if (b.ncomp <= 0)
     return cudaSuccess;
   EnoTiling t;
@@ -357,8 +384,8 @@ cudaError_t launch_eno_cell_box(const BoxDesc &b, int per_group, signed char *sh
     if (b.rhi[d] < b.rlo[d])
       return cudaSuccess;
     t.clo[d] = b.rlo[d] >> 1;
-    const int ncell = (b.rhi[d] >> 1) - t.clo[d] + 1;
-    t.nt[d] = (ncell + ET - 1) / ET;
+    t.nc[d] = (b.rhi[d] >> 1) - t.clo[d] + 1;
+    t.nt[d] = (t.nc[d] + ET - 1) / ET;
   }
   t.nblk = per_group ? 1 : b.ncomp;
   const int64_t n = (int64_t)t.nt[0] * t.nt[1] * t.nt[2] * t.nblk;
@@ -367,14 +394,19 @@ cudaError_t launch_eno_cell_box(const BoxDesc &b, int per_group, signed char *sh
   const int dev = cache_device();
   int grid = dev >= 0 ? g_eno_grid[dev].load() : 0;
   if (!grid) {
-    cudaError_t e = cudaFuncSetAttribute(eno_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(eno_cell_kernel<false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)sizeof(EnoShared));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(eno_cell_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(EnoShared));
     if (e != cudaSuccess)
       return e;
     int per_sm = 0, d = 0, sms = 0;
     cudaGetDevice(&d);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eno_cell_kernel, ENT, sizeof(EnoShared));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eno_cell_kernel<false>, ENT,
+                                                  sizeof(EnoShared));
     grid = sms * (per_sm > 0 ? per_sm : 1);
     if (dev >= 0)
       g_eno_grid[dev].store(grid);
@@ -389,7 +421,195 @@ cudaError_t launch_eno_cell_box(const BoxDesc &b, int per_group, signed char *sh
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
   cfg.numAttrs = after_level ? 1 : 0;
-  return cudaLaunchKernelEx(&cfg, eno_cell_kernel, b, t, per_group, shifts, fallback);
+  if (cshift)
+    return cudaLaunchKernelEx(&cfg, eno_cell_kernel<true>, b, t, per_group, shifts, fallback,
+                              cshift);
+  return cudaLaunchKernelEx(&cfg, eno_cell_kernel<false>, b, t, per_group, shifts, fallback,
+                            cshift);
+}
+
+
+namespace {
+
+// Adjoint of the ENO-per-cell operators, linearised at the coarse input:
+// fine point f = 2 p + o (o in {0,1}^3) of parent cell p with shift s reads
+// coarse p + s + (a - 1) with weight wx(sx, ox, ax) wy(sy, oy, ay)
+// wz(sz, oz, az) (interp1d<CC,ENO,2>'s row, impl.hxx:806-841), so
+//   crse_bar(q) = sum over parents p with t = q - p - s in [-1, 1]^3 of
+//                 sum_o wz(oz, tz + 1) wy(oy, ty + 1) wx(ox, tx + 1) fbar(2 p + o),
+// fine points outside the region counting as 0.  A CTA takes a tile of
+// AX x AY x AZ coarse points of the coarse box (one thread each) and stages
+// the shift codes of the parents within 2 cells (the decision pass's
+// cshift) and their children's fine_bar in shared memory; every coarse
+// point scans its 125 candidate parents in a fixed order (no atomics,
+// deterministic) and writes its value, zero where no region point reads it.
+constexpr int AX = 8, AY = 8, AZ = 4;
+constexpr int PWX = AX + 4, PWY = AY + 4, PWZ = AZ + 4; // parent window
+constexpr int FWX = 2 * PWX, FWY = 2 * PWY, FWZ = 2 * PWZ; // the parents' children
+constexpr int ANT = AX * AY * AZ;
+
+struct EnoAdjShared {
+  double f[FWZ * FWY * FWX];
+  // per parent: the offsets d = p - q it serves, bit d_x + 2, d_y + 7,
+  // d_z + 12 (d_i + s_i in [-1, 1]: three consecutive bits from 1 - s_i per
+  // direction, so s_i = 1 - (lowest set bit of its field)); 0: no children
+  // in the region
+  unsigned short code[PWZ * PWY * PWX];
+};
+
+__constant__ double c_eno_w[3][2][3]; // [shift + 1][off][tap]
+
+__global__ void __launch_bounds__(ANT)
+    eno_adjoint_kernel(const __grid_constant__ BoxDesc b, const EnoTiling t, int per_group,
+                       const unsigned char *__restrict__ cshift, double *__restrict__ cbar,
+                       int ntx, int nty) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  EnoAdjShared &sh = *reinterpret_cast<EnoAdjShared *>(smem_raw);
+  const int tid = threadIdx.x;
+  const int blk = blockIdx.y;
+  const int tile = blockIdx.x;
+  const int cnz = (int)(b.cnp / ((int64_t)b.cnx * b.cny));
+  const int q0x = b.clo[0] + (tile % ntx) * AX, q0y = b.clo[1] + ((tile / ntx) % nty) * AY,
+            q0z = b.clo[2] + (tile / (ntx * nty)) * AZ;
+  const int64_t ncell = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+  // parents p = q0 - 2 + (i, j, k)
+  for (int e = tid; e < PWX * PWY * PWZ; e += ANT) {
+    const int i = e % PWX, j = (e / PWX) % PWY, k = e / (PWX * PWY);
+    const int lx = q0x - 2 + i - t.clo[0], ly = q0y - 2 + j - t.clo[1], lz = q0z - 2 + k - t.clo[2];
+    unsigned int w = 0;
+    if (lx >= 0 && lx < t.nc[0] && ly >= 0 && ly < t.nc[1] && lz >= 0 && lz < t.nc[2]) {
+      const int c = cshift[blk * ncell + lx + (int64_t)t.nc[0] * (ly + (int64_t)t.nc[1] * lz)];
+      const int sx = c % 3 - 1, sy = (c / 3) % 3 - 1, sz = c / 9 - 1;
+      w = (7u << (1 - sx)) | (7u << (6 - sy)) | (7u << (11 - sz));
+    }
+    sh.code[e] = (unsigned short)w;
+  }
+  const int ix = tid % AX, iy = (tid / AX) % AY, iz = tid / (AX * AY);
+  const int qx = q0x + ix, qy = q0y + iy, qz = q0z + iz;
+  const bool mine = qx < b.clo[0] + b.cnx && qy < b.clo[1] + b.cny && qz < b.clo[2] + cnz;
+  const int c0 = per_group ? 0 : blk, c1 = per_group ? b.ncomp : blk + 1;
+  const int64_t fplane = (int64_t)b.fnx * b.fny;
+  const int fx0 = 2 * (q0x - 2), fy0 = 2 * (q0y - 2), fz0 = 2 * (q0z - 2);
+  for (int comp = c0; comp < c1; ++comp) {
+    __syncthreads(); // the codes are written; the previous component's f is read
+    const double *fb = b.fine + comp * b.fnp;
+    for (int e = tid; e < FWX * FWY * FWZ; e += ANT) {
+      const int i = e % FWX, j = (e / FWX) % FWY, k = e / (FWX * FWY);
+      const int fx = fx0 + i, fy = fy0 + j, fz = fz0 + k;
+      double v = 0.0;
+      if (fx >= b.rlo[0] && fx <= b.rhi[0] && fy >= b.rlo[1] && fy <= b.rhi[1] &&
+          fz >= b.rlo[2] && fz <= b.rhi[2])
+        v = fb[(fx - b.flo[0]) + (int64_t)b.fnx * (fy - b.flo[1]) + fplane * (fz - b.flo[2])];
+      sh.f[e] = v;
+    }
+    __syncthreads();
+    if (!mine)
+      continue;
+    double acc = 0.0;
+    const unsigned short *cbase = sh.code + (ix + 2) + PWX * ((iy + 2) + PWY * (iz + 2));
+#pragma unroll 1
+    for (int dz = -2; dz <= 2; ++dz)
+#pragma unroll 1
+      for (int dy = -2; dy <= 2; ++dy)
+#pragma unroll
+        for (int dx = -2; dx <= 2; ++dx) {
+          // parent p = q + d
+          const unsigned int w = cbase[dx + PWX * (dy + PWY * dz)];
+          const unsigned int want = (1u << (dx + 2)) | (1u << (dy + 7)) | (1u << (dz + 12));
+          if ((w & want) != want)
+            continue;
+          // lowest set bit of each field: 1 - s_i; the tap a_i = 1 - s_i - d_i
+          const int lx = __ffs(w & 31u) - 1, ly = __ffs((w >> 5) & 31u) - 1,
+                    lz = __ffs((w >> 10) & 31u) - 1;
+          const int sx = 1 - lx, sy = 1 - ly, sz = 1 - lz;
+          const int ax = lx - dx, ay = ly - dy, az = lz - dz; // taps, in 0..2
+          // the children 2 p + o, fine local 2 (p local) + o
+          const double *f = sh.f + 2 * (ix + 2 + dx) + FWX * (2 * (iy + 2 + dy) +
+                                                               FWY * 2 * (iz + 2 + dz));
+          double sz_ = 0.0;
+#pragma unroll
+          for (int oz = 0; oz < 2; ++oz) {
+            double sy_ = 0.0;
+#pragma unroll
+            for (int oy = 0; oy < 2; ++oy) {
+              const double *r = f + FWX * (oy + FWY * oz);
+              const double sx_ = fma(c_eno_w[sx + 1][1][ax], r[1], c_eno_w[sx + 1][0][ax] * r[0]);
+              sy_ = fma(c_eno_w[sy + 1][oy][ay], sx_, sy_);
+            }
+            sz_ = fma(c_eno_w[sz + 1][oz][az], sy_, sz_);
+          }
+          acc += sz_;
+        }
+    cbar[comp * b.cnp + (qx - b.clo[0]) + (int64_t)b.cnx * (qy - b.clo[1]) +
+         (int64_t)b.cnx * b.cny * (qz - b.clo[2])] = acc;
+  }
+}
+
+std::atomic<bool> g_eno_w_set[kMaxDevices];
+
+} // namespace
+
+size_t eno_adjoint_scratch_bytes(const BoxDesc &b, int per_group) {
+  int64_t n = per_group ? 1 : b.ncomp;
+  for (int d = 0; d < 3; ++d) {
+    if (b.rhi[d] < b.rlo[d])
+      return 0;
+    n *= (b.rhi[d] >> 1) - (b.rlo[d] >> 1) + 1;
+  }
+  return (size_t)n;
+}
+
+cudaError_t launch_eno_adjoint_box(const BoxDesc &b, int per_group, void *scratch,
+                                   double *crse_bar, cudaStream_t s) {
+  if (b.ncomp <= 0 || b.cnp <= 0)
+    return cudaSuccess;
+  EnoTiling t;
+  bool empty = false;
+  for (int d = 0; d < 3; ++d) {
+    empty = empty || b.rhi[d] < b.rlo[d];
+    t.clo[d] = b.rlo[d] >> 1;
+    t.nc[d] = empty ? 0 : (b.rhi[d] >> 1) - t.clo[d] + 1;
+    t.nt[d] = 0;
+  }
+  t.nblk = per_group ? 1 : b.ncomp;
+  unsigned char *cs = static_cast<unsigned char *>(scratch);
+  const int dev = cache_device();
+  if (dev < 0 || !g_eno_w_set[dev].load()) {
+    double w[3][2][3];
+    for (int sh = -1; sh <= 1; ++sh)
+      for (int off = 0; off < 2; ++off) {
+        const int m = off == 0 ? sh + 1 : 1 - sh;
+        for (int i = 0; i < 3; ++i) {
+          const int j = off == 0 ? i : 2 - i;
+          w[sh + 1][off][i] = cc_eno2_c(m, j);
+        }
+      }
+    cudaError_t e = cudaMemcpyToSymbol(c_eno_w, w, sizeof w);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(eno_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(EnoAdjShared));
+    if (e != cudaSuccess)
+      return e;
+    if (dev >= 0)
+      g_eno_w_set[dev].store(true);
+  }
+  if (!empty) {
+    // the decisions: one shift code per coarse cell with children in the region
+    BoxDesc d = b;
+    d.fine = nullptr;
+    if (cudaError_t e = launch_eno_cell_box(d, per_group, nullptr, nullptr, s, false, cs))
+      return e;
+  }
+  const int cnz = (int)(b.cnp / ((int64_t)b.cnx * b.cny));
+  const int ntx = (b.cnx + AX - 1) / AX, nty = (b.cny + AY - 1) / AY, ntz = (cnz + AZ - 1) / AZ;
+  const int64_t ntiles = (int64_t)ntx * nty * ntz;
+  if (ntiles > INT32_MAX)
+    return cudaErrorInvalidValue;
+  if (empty) // nothing reads the coarse box: zero
+    return cudaMemsetAsync(crse_bar, 0, sizeof(double) * b.cnp * b.ncomp, s);
+  eno_adjoint_kernel<<<dim3((unsigned)ntiles, t.nblk), ANT, sizeof(EnoAdjShared), s>>>(
+      b, t, per_group, cs, crse_bar, ntx, nty);
+  return cudaGetLastError();
 }
 
 } // namespace cxb

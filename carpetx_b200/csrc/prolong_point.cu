@@ -446,6 +446,8 @@ cudaError_t launch_point_box(const BoxDesc &b, int per_group, signed char *shift
 // (3 bytes) and fallback flag (1 byte) of every region point and component
 // block, when it has ENO directions or an active linear fallback; else 0.
 size_t point_adjoint_scratch_bytes(const BoxDesc &b, int per_group) {
+  if (eno_cell_applies(b, per_group))
+    return eno_adjoint_scratch_bytes(b, per_group);
   const int64_t rnp = (int64_t)(b.rhi[0] - b.rlo[0] + 1) * (b.rhi[1] - b.rlo[1] + 1) *
                       (b.rhi[2] - b.rlo[2] + 1);
   bool eno = false;
@@ -464,6 +466,8 @@ cudaError_t launch_point_adjoint_box_scratch(const BoxDesc &b, int per_group, do
                                              void *scratch, cudaStream_t s) {
   if (b.ncomp <= 0 || b.cnp <= 0)
     return cudaSuccess;
+  if (eno_cell_applies(b, per_group)) // all directions ENO: per-cell shifts, tiled gather
+    return launch_eno_adjoint_box(b, per_group, scratch, crse_bar, s);
   const int nblk = per_group ? 1 : b.ncomp;
   const size_t need = point_adjoint_scratch_bytes(b, per_group);
   signed char *sh = nullptr;
