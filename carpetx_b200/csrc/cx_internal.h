@@ -123,6 +123,11 @@ cudaError_t launch_eno_cell_box(const BoxDesc &b, int per_group, signed char *sh
 size_t eno_adjoint_scratch_bytes(const BoxDesc &b, int per_group);
 cudaError_t launch_eno_adjoint_box(const BoxDesc &b, int per_group, void *scratch,
                                    double *crse_bar, cudaStream_t s);
+// Adjoint of the CCC minmod operator (minmod in all three directions) on one
+// box: the forward's choices recomputed per tile, three transposed passes in
+// shared memory; no scratch.
+bool minmod_cell_applies(const BoxDesc &b);
+cudaError_t launch_minmod_adjoint_box(const BoxDesc &b, double *crse_bar, cudaStream_t s);
 cudaError_t launch_point_level(const BoxDesc *d_boxes, const TileRef *d_tiles,
                                int ntiles, int per_group, cudaStream_t s);
 

@@ -468,6 +468,8 @@ cudaError_t launch_point_adjoint_box_scratch(const BoxDesc &b, int per_group, do
     return cudaSuccess;
   if (eno_cell_applies(b, per_group)) // all directions ENO: per-cell shifts, tiled gather
     return launch_eno_adjoint_box(b, per_group, scratch, crse_bar, s);
+  if (minmod_cell_applies(b)) // all directions minmod: tiled transposed passes
+    return launch_minmod_adjoint_box(b, crse_bar, s);
   const int nblk = per_group ? 1 : b.ncomp;
   const size_t need = point_adjoint_scratch_bytes(b, per_group);
   signed char *sh = nullptr;

@@ -187,3 +187,48 @@ def test_gpu_shock_minmod_matches_oracle(dev, cx):
         torch.cuda.synchronize()
         plan.close()
         assert_bitwise(got.cpu().numpy(), want, f"minmod, box {bid}")
+
+
+@pytest.mark.parametrize("typ,order,sub", [("eno", 3, True), ("minmod", 1, False)])
+def test_gpu_shock_limited_adjoint_matches_oracle(dev, cx, typ, order, sub):
+    """The limited adjoints of the shock configuration at full size: one box
+    of 64^3 coarse cells that the shock crosses, through the adjoint level
+    plan linearised at the box's coarse data, against the oracle's transpose
+    (within roundoff) and the dot-product identity <P(u), v> = <u, P'(u)^T v>.
+    Minmod: the whole box, 5 variables.  ENO (whose oracle transpose is
+    slow): a 64^3 fine region off the box's corner, across tile seams, 2
+    variables."""
+    state, boxes = _shock_boxes(1)
+    op = cb.Op(typ, order, 7)
+    rng = np.random.default_rng(77)
+    for bid, clo, chi, flo, fhi in boxes:
+        nc = 2 if sub else 5
+        crse = np.ascontiguousarray(shock_fab(state, clo, chi, bid)[:nc])
+        rlo, rhi = flo, fhi
+        if sub:
+            rlo = tuple(flo[d] + 37 for d in range(3))
+            rhi = tuple(rlo[d] + 63 for d in range(3))
+        mask = np.zeros((1,) + box_shape(flo, fhi))
+        mask[0, rlo[2] - flo[2]:rhi[2] - flo[2] + 1, rlo[1] - flo[1]:rhi[1] - flo[1] + 1,
+             rlo[0] - flo[0]:rhi[0] - flo[0] + 1] = 1.0
+        v = rng.standard_normal((nc,) + box_shape(flo, fhi)) * mask
+        want = np.zeros_like(crse)
+        cx.prolong_adjoint(typ, order, 7, 0, crse, clo, chi, v, flo, fhi, rlo, rhi, nc, want)
+        got = torch.full(crse.shape, np.nan, dtype=torch.float64, device="cuda")
+        g_crse = torch.from_numpy(crse).cuda()
+        plan = cb.LevelPlan([dict(op=op, ncomp=nc, crse=got, crse_at=g_crse, crse_lo=clo,
+                                  crse_hi=chi, fine=torch.from_numpy(v).cuda(), fine_lo=flo,
+                                  fine_hi=fhi, reg_lo=rlo, reg_hi=rhi)], adjoint=True)
+        plan.execute()
+        pu = torch.zeros(v.shape, dtype=torch.float64, device="cuda")
+        cb.prolong_box(op, g_crse, clo, chi, pu, flo, fhi, rlo, rhi, nc)
+        torch.cuda.synchronize()
+        plan.close()
+        assert cb.lib().cx_check_device() == cb.CX_OK
+        g = got.cpu().numpy()
+        scale = max(1.0, np.abs(want).max())
+        np.testing.assert_allclose(g, want, rtol=1e-12, atol=1e-12 * scale,
+                                   err_msg=f"{typ} adjoint, box {bid}")
+        lhs = float(np.sum(pu.cpu().numpy() * v))
+        rhs = float(np.sum(crse * g))
+        assert abs(lhs - rhs) <= 1e-12 * np.sum(np.abs(crse * g)), (typ, lhs, rhs)
