@@ -65,6 +65,7 @@ METRIC = "FP64 fine points/s, batched persistent level prolongation"
 UNIT = "fine points/s"
 L2_BYTES = 126 * 1024 * 1024
 E2E_BATCHES = 8  # box batches of the end-to-end leg's copy/transfer pipeline
+E2E_CHUNK_MB = 0  # largest single copy of that pipeline, MB (0: one copy per batch)
 # ncu DRAM bytes per fine point of the level512 workload's step (the eight
 # separable kernels), from a capture of the same 512 boxes with 2 components
 # instead of 24 (1/12 of the fine points) with --cache-control none, so that
@@ -85,12 +86,18 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--per-box-steps", type=int, default=2)
     p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--e2e-batches", type=int, default=E2E_BATCHES,
+                   help="e2e: batches of consecutive boxes, one plan each")
+    p.add_argument("--e2e-chunk-mb", type=int, default=E2E_CHUNK_MB,
+                   help="e2e: largest single host <-> device copy, MB (0: one per batch)")
     p.add_argument("--adjoint-steps", type=int, default=3,
                    help="passes of the forward/adjoint comparison (0: skip)")
     p.add_argument("--restrict-steps", type=int, default=5,
                    help="passes of the restriction leg (0: skip)")
     p.add_argument("--limited-steps", type=int, default=2,
                    help="passes of the ENO / minmod leg (0: skip)")
+    p.add_argument("--limited-boxes", type=int, default=64,
+                   help="boxes of the shock level the ENO / minmod leg takes (at most 64)")
     p.add_argument("--halo-steps", type=int, default=5,
                    help="executions of the halo-exchange leg (0: skip)")
     p.add_argument("--boundary-steps", type=int, default=5,
@@ -355,7 +362,7 @@ def limited_leg(args, cb, torch, dev, max_over_ranks, barrier):
     from carpetx_b200.workloads import shock_fab, shock_level_boxes, shock_state
     nc = 5
     state = shock_state(args.seed + 4, 256)
-    sboxes = shock_level_boxes()
+    sboxes = shock_level_boxes()[:max(1, args.limited_boxes)]
     nb = len(sboxes)
     flo0, fhi0 = sboxes[0][3], sboxes[0][4]
     out = {"workload": f"{nb} boxes, 64^3 coarse cells -> 128^3 fine, {nc} vars (rho, momenta, "
@@ -404,10 +411,11 @@ def limited_leg(args, cb, torch, dev, max_over_ranks, barrier):
             aplan.execute()
             barrier()
             e0.record()
-            aplan.execute()
+            for _ in range(args.limited_steps):
+                aplan.execute()
             e1.record()
             barrier()
-            ms_a = max_over_ranks(e0.elapsed_time(e1))
+            ms_a = max_over_ranks(e0.elapsed_time(e1)) / args.limited_steps
             out[f"{typ}_adjoint_ms"] = ms_a
             out[f"{typ}_adjoint_over_forward"] = ms_a / ms
             aplan.close()
@@ -1057,19 +1065,27 @@ def main():
 
     # end to end through the C ABI with host buffers: every step copies all
     # coarse data in from pinned host memory and all fine data out.  The
-    # level is split into E2E_BATCHES batches of consecutive boxes, one plan
+    # level is split into --e2e-batches batches of consecutive boxes, one plan
     # each, pipelined over three streams: batch k's copy in, transfer and
     # copy out wait for each other, and the copy in (copy out) of a batch
     # waits for the previous step's transfer (copy out) of that batch, whose
     # buffers it overwrites.  Copies in and out then run at the same time on
-    # the two copy directions, beside the transfers.
+    # the two copy directions, beside the transfers.  Each batch's copies are
+    # issued in pieces of at most --e2e-chunk-mb.
     ms_e2e, e2e_value = None, None
     if args.e2e_steps > 0:
         h_crse = torch.empty(ctot, dtype=torch.float64, pin_memory=True)
         h_fine = torch.empty(ftot, dtype=torch.float64, pin_memory=True)
         h_crse.copy_(crse.cpu())
         nb = len(lb)
-        cuts = sorted({round(i * nb / E2E_BATCHES) for i in range(E2E_BATCHES + 1)})
+        nbat = max(1, args.e2e_batches)
+        cuts = sorted({round(i * nb / nbat) for i in range(nbat + 1)})
+        chunk = args.e2e_chunk_mb * (1 << 20) // 8 if args.e2e_chunk_mb > 0 else None
+
+        def copy_chunks(dst, src, a, z):
+            step = chunk or (z - a)
+            for u in range(a, z, step):
+                dst[u:min(u + step, z)].copy_(src[u:min(u + step, z)], non_blocking=True)
         coff_all, foff_all = coff + [ctot], foff + [ftot]
         batches = [(cb.LevelPlan(lb[a:z]), coff_all[a], coff_all[z], foff_all[a], foff_all[z])
                    for a, z in zip(cuts[:-1], cuts[1:]) if z > a]
@@ -1083,7 +1099,7 @@ def main():
                 with torch.cuda.stream(s_in):
                     if done_x[k] is not None:
                         s_in.wait_event(done_x[k])
-                    crse[c0:c1].copy_(h_crse[c0:c1], non_blocking=True)
+                    copy_chunks(crse, h_crse, c0, c1)
                     ev_in.record(s_in)
                 stream.wait_event(ev_in)
                 if done_o[k] is not None:
@@ -1092,7 +1108,7 @@ def main():
                 ev_x.record(stream)
                 with torch.cuda.stream(s_out):
                     s_out.wait_event(ev_x)
-                    h_fine[f0:f1].copy_(fine[f0:f1], non_blocking=True)
+                    copy_chunks(h_fine, fine, f0, f1)
                     ev_o.record(s_out)
                 done_x[k], done_o[k] = ev_x, ev_o
 
@@ -1155,7 +1171,8 @@ def main():
                     "timing": "one CUDA graph of the per-box launches, replayed",
                     "batched_speedup": value / per_box_value if per_box_value else None},
         "e2e": {"value": e2e_value, "unit": UNIT, "ms_per_step": ms_e2e,
-                "h2d_bytes_per_step": 8 * ctot, "d2h_bytes_per_step": 8 * ftot},
+                "h2d_bytes_per_step": 8 * ctot, "d2h_bytes_per_step": 8 * ftot,
+                "batches": args.e2e_batches, "copy_chunk_mb": args.e2e_chunk_mb},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "traffic_unit": "bytes per step (rank 0)",

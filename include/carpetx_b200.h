@@ -191,9 +191,10 @@ int cx_level_plan_create_adjoint(const cx_box_t *boxes, int nboxes,
  * be null for linear operators).  As cx_prolong_adjoint_box, P^T is taken
  * with each fine point's choices (ENO shift, minmod branch, linear fallback)
  * recomputed from crse_at: after the streaming launches, every box of a
- * limited operator takes a decision pass into scratch the plan allocates
- * once, then a gather.  Executions of one plan must not overlap (the
- * scratch is the plan's). */
+ * limited operator takes its own launches (CCC minmod: one tiled kernel that
+ * recomputes the choices; the others: a decision pass into scratch the plan
+ * allocates once, then a gather).  Executions of one plan must not overlap
+ * (the scratch is the plan's). */
 int cx_level_plan_create_adjoint_at(const cx_box_t *boxes, const double *const *crse_at,
                                     int nboxes, int per_group, cx_level_plan_t *out);
 
