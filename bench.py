@@ -92,6 +92,10 @@ def parse():
                    help="e2e: largest single host <-> device copy, MB (0: one per batch)")
     p.add_argument("--adjoint-steps", type=int, default=3,
                    help="passes of the forward/adjoint comparison (0: skip)")
+    p.add_argument("--adjoint-boxes", type=int, default=64,
+                   help="boxes of the adjoint leg's level (64: the differentiated configuration)")
+    p.add_argument("--adjoint-batch", type=int, default=16,
+                   help="levels of the adjoint leg's streamed batch (0: skip the batch)")
     p.add_argument("--restrict-steps", type=int, default=5,
                    help="passes of the restriction leg (0: skip)")
     p.add_argument("--limited-steps", type=int, default=2,
@@ -148,6 +152,8 @@ def adjoint_leg(args, cb, torch, dev, max_over_ranks, barrier):
     boxes = []
     for i in range(64):
         n = np.round(np.exp(rng.uniform(np.log(32), np.log(96), 3))).astype(int)
+        if i >= args.adjoint_boxes:
+            continue
         typ, order, it = ("interpolate", 5, 0) if i % 2 == 0 else ("conservative", 1, 7)
         cc = 1 if it == 7 else 0
         flo = (0, 0, 0)
@@ -181,7 +187,7 @@ def adjoint_leg(args, cb, torch, dev, max_over_ranks, barrier):
 
     plan_f = cb.LevelPlan(plan_boxes(False))
     plan_a = cb.LevelPlan(plan_boxes(True), adjoint=True)
-    out = {"workload": "64 boxes, coarse 32-96 points/dim log-uniform, 4 vars, interpolate o5 VVV "
+    out = {"workload": f"{len(boxes)} boxes, coarse 32-96 points/dim log-uniform, 4 vars, interpolate o5 VVV "
                        "/ conservative o1 CCC; level plans (one persistent launch per stencil "
                        "pair) and one launch per box",
            "fine_points": nfine}
@@ -203,7 +209,9 @@ def adjoint_leg(args, cb, torch, dev, max_over_ranks, barrier):
     plan_f.close()
     plan_a.close()
     del data
-    out["batch16"] = adjoint_batch(args, cb, torch, dev, max_over_ranks, barrier, nc)
+    if args.adjoint_batch > 0:
+        out["batch16"] = adjoint_batch(args, cb, torch, dev, max_over_ranks, barrier, nc,
+                                       args.adjoint_batch)
     return out
 
 
