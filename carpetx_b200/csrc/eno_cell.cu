@@ -434,32 +434,40 @@ namespace {
 // Adjoint of the ENO-per-cell operators, linearised at the coarse input:
 // fine point f = 2 p + o (o in {0,1}^3) of parent cell p with shift s reads
 // coarse p + s + (a - 1) with weight wx(sx, ox, ax) wy(sy, oy, ay)
-// wz(sz, oz, az) (interp1d<CC,ENO,2>'s row, impl.hxx:806-841), so
-//   crse_bar(q) = sum over parents p with t = q - p - s in [-1, 1]^3 of
-//                 sum_o wz(oz, tz + 1) wy(oy, ty + 1) wx(ox, tx + 1) fbar(2 p + o),
-// fine points outside the region counting as 0.  A CTA takes a tile of
-// AX x AY x AZ coarse points of the coarse box (one thread each) and stages
-// the shift codes of the parents within 2 cells (the decision pass's
-// cshift) and their children's fine_bar in shared memory; every coarse
-// point scans its 125 candidate parents in a fixed order (no atomics,
-// deterministic) and writes its value, zero where no region point reads it.
+// wz(sz, oz, az) (interp1d<CC,ENO,2>'s row, impl.hxx:806-841), so parent p
+// adds to coarse q = p + s + a - 1 its tap contribution
+//   W(p, a) = sum_o wz(sz, oz, az) wy(sy, oy, ay) wx(sx, ox, ax) fbar(2 p + o),
+// fine points outside the region counting as 0, and
+//   crse_bar(q) = sum over parents p with a = q - p - s + 1 in [0, 2]^3 of W(p, a).
+// A CTA takes a tile of AX x AY x AZ coarse points of the coarse box (one
+// thread each), stages the shift codes of the parents within 2 cells (the
+// decision pass's cshift) once, and walks the parents' z planes: per plane it
+// stages the two fine planes of the children, every parent of the plane
+// computes its 27 contributions (x, then y, then z contraction) into shared
+// memory, and every coarse point within two planes adds those of its
+// matching candidate parents (25 per plane, one mask test each).  The order
+// of the sums is fixed (no atomics, deterministic); every coarse point of
+// the box is written, zero where no region point reads it.
 constexpr int AX = 8, AY = 8, AZ = 4;
 constexpr int PWX = AX + 4, PWY = AY + 4, PWZ = AZ + 4; // parent window
-constexpr int FWX = 2 * PWX, FWY = 2 * PWY, FWZ = 2 * PWZ; // the parents' children
+constexpr int PWXY = PWX * PWY;
+constexpr int FWX = 2 * PWX, FWY = 2 * PWY;             // the children of a parent plane
 constexpr int ANT = AX * AY * AZ;
 
 struct EnoAdjShared {
-  double f[FWZ * FWY * FWX];
+  double f[2][2][FWY * FWX]; // fine_bar of a parent plane's children [buffer][oz][fy][fx]
+  double w[27][PWXY];      // W(p, a) of the plane's parents [a][parent]
+  double tw[3][2][3];      // interp1d<CC,ENO,2> weights [shift + 1][off][tap]
   // per parent: the offsets d = p - q it serves, bit d_x + 2, d_y + 7,
   // d_z + 12 (d_i + s_i in [-1, 1]: three consecutive bits from 1 - s_i per
   // direction, so s_i = 1 - (lowest set bit of its field)); 0: no children
   // in the region
-  unsigned short code[PWZ * PWY * PWX];
+  unsigned short code[PWZ * PWXY];
 };
 
 __constant__ double c_eno_w[3][2][3]; // [shift + 1][off][tap]
 
-__global__ void __launch_bounds__(ANT)
+__global__ void __launch_bounds__(ANT, 3)
     eno_adjoint_kernel(const __grid_constant__ BoxDesc b, const EnoTiling t, int per_group,
                        const unsigned char *__restrict__ cshift, double *__restrict__ cbar,
                        int ntx, int nty) {
@@ -472,9 +480,11 @@ __global__ void __launch_bounds__(ANT)
   const int q0x = b.clo[0] + (tile % ntx) * AX, q0y = b.clo[1] + ((tile / ntx) % nty) * AY,
             q0z = b.clo[2] + (tile / (ntx * nty)) * AZ;
   const int64_t ncell = (int64_t)t.nc[0] * t.nc[1] * t.nc[2];
+  if (tid < 18)
+    (&sh.tw[0][0][0])[tid] = (&c_eno_w[0][0][0])[tid];
   // parents p = q0 - 2 + (i, j, k)
   for (int e = tid; e < PWX * PWY * PWZ; e += ANT) {
-    const int i = e % PWX, j = (e / PWX) % PWY, k = e / (PWX * PWY);
+    const int i = e % PWX, j = (e / PWX) % PWY, k = e / PWXY;
     const int lx = q0x - 2 + i - t.clo[0], ly = q0y - 2 + j - t.clo[1], lz = q0z - 2 + k - t.clo[2];
     unsigned int w = 0;
     if (lx >= 0 && lx < t.nc[0] && ly >= 0 && ly < t.nc[1] && lz >= 0 && lz < t.nc[2]) {
@@ -489,60 +499,97 @@ __global__ void __launch_bounds__(ANT)
   const bool mine = qx < b.clo[0] + b.cnx && qy < b.clo[1] + b.cny && qz < b.clo[2] + cnz;
   const int c0 = per_group ? 0 : blk, c1 = per_group ? b.ncomp : blk + 1;
   const int64_t fplane = (int64_t)b.fnx * b.fny;
-  const int fx0 = 2 * (q0x - 2), fy0 = 2 * (q0y - 2), fz0 = 2 * (q0z - 2);
-  for (int comp = c0; comp < c1; ++comp) {
-    __syncthreads(); // the codes are written; the previous component's f is read
+  const int fx0 = 2 * (q0x - 2), fy0 = 2 * (q0y - 2);
+  // the children of parent plane k of component comp into buffer buf:
+  // asynchronous 8-byte copies, zero outside the region
+  auto stage = [&](int comp, int k, int buf) {
     const double *fb = b.fine + comp * b.fnp;
-    for (int e = tid; e < FWX * FWY * FWZ; e += ANT) {
-      const int i = e % FWX, j = (e / FWX) % FWY, k = e / (FWX * FWY);
-      const int fx = fx0 + i, fy = fy0 + j, fz = fz0 + k;
-      double v = 0.0;
-      if (fx >= b.rlo[0] && fx <= b.rhi[0] && fy >= b.rlo[1] && fy <= b.rhi[1] &&
-          fz >= b.rlo[2] && fz <= b.rhi[2])
-        v = fb[(fx - b.flo[0]) + (int64_t)b.fnx * (fy - b.flo[1]) + fplane * (fz - b.flo[2])];
-      sh.f[e] = v;
+    for (int e = tid; e < 2 * FWX * FWY; e += ANT) {
+      const int i = e % FWX, j = (e / FWX) % FWY, oz = e / (FWX * FWY);
+      const int fx = fx0 + i, fy = fy0 + j, fz = 2 * (q0z - 2 + k) + oz;
+      const bool ok = fx >= b.rlo[0] && fx <= b.rhi[0] && fy >= b.rlo[1] && fy <= b.rhi[1] &&
+                      fz >= b.rlo[2] && fz <= b.rhi[2];
+      const double *src =
+          ok ? fb + (fx - b.flo[0]) + (int64_t)b.fnx * (fy - b.flo[1]) + fplane * (fz - b.flo[2])
+             : fb;
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(
+                       (unsigned)__cvta_generic_to_shared(&sh.f[buf][oz][j * FWX + i])),
+                   "l"(src), "r"(ok ? 8 : 0)
+                   : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  const int nit = (c1 - c0) * PWZ; // (component, parent plane) steps
+  stage(c0, 0, 0);
+  double acc = 0.0;
+  for (int it = 0; it < nit; ++it) {
+    const int comp = c0 + it / PWZ, k = it % PWZ, buf = it & 1; // parent plane q0z - 2 + k
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads(); // this plane's children are in; the previous plane is consumed
+    if (it + 1 < nit)
+      stage(c0 + (it + 1) / PWZ, (it + 1) % PWZ, buf ^ 1);
+    // the plane's parents: W(p, a), x then y then z contraction
+    for (int e = tid; e < PWXY; e += ANT) {
+      const unsigned int w = sh.code[k * PWXY + e];
+      if (!w)
+        continue; // no children in the region: never matched
+      const int pi = e % PWX, pj = e / PWX;
+      const int sx = 2 - __ffs(w & 31u), sy = 2 - __ffs((w >> 5) & 31u),
+                sz = 2 - __ffs((w >> 10) & 31u);
+      const double *wx = sh.tw[sx + 1][0], *wy = sh.tw[sy + 1][0], *wz = sh.tw[sz + 1][0];
+      double uy[2][3][3]; // [oz][ay][ax]
+#pragma unroll
+      for (int oz = 0; oz < 2; ++oz) {
+        double ux[2][3]; // [oy][ax]
+#pragma unroll
+        for (int oy = 0; oy < 2; ++oy) {
+          const double *r = sh.f[buf][oz] + (2 * pj + oy) * FWX + 2 * pi;
+          const double r0 = r[0], r1 = r[1];
+#pragma unroll
+          for (int ax = 0; ax < 3; ++ax)
+            ux[oy][ax] = fma(wx[3 + ax], r1, wx[ax] * r0);
+        }
+#pragma unroll
+        for (int ay = 0; ay < 3; ++ay)
+#pragma unroll
+          for (int ax = 0; ax < 3; ++ax)
+            uy[oz][ay][ax] = fma(wy[3 + ay], ux[1][ax], wy[ay] * ux[0][ax]);
+      }
+#pragma unroll
+      for (int az = 0; az < 3; ++az)
+#pragma unroll
+        for (int ay = 0; ay < 3; ++ay)
+#pragma unroll
+          for (int ax = 0; ax < 3; ++ax)
+            sh.w[(az * 3 + ay) * 3 + ax][e] =
+                fma(wz[3 + az], uy[1][ay][ax], wz[az] * uy[0][ay][ax]);
     }
     __syncthreads();
-    if (!mine)
-      continue;
-    double acc = 0.0;
-    const unsigned short *cbase = sh.code + (ix + 2) + PWX * ((iy + 2) + PWY * (iz + 2));
-#pragma unroll 1
-    for (int dz = -2; dz <= 2; ++dz)
+    const int dz = k - 2 - iz; // p_z - q_z, uniform per warp
+    if (mine && dz >= -2 && dz <= 2) {
 #pragma unroll 1
       for (int dy = -2; dy <= 2; ++dy)
 #pragma unroll
         for (int dx = -2; dx <= 2; ++dx) {
-          // parent p = q + d
-          const unsigned int w = cbase[dx + PWX * (dy + PWY * dz)];
+          const int pe = (iy + 2 + dy) * PWX + (ix + 2 + dx);
+          const unsigned int w = sh.code[k * PWXY + pe];
           const unsigned int want = (1u << (dx + 2)) | (1u << (dy + 7)) | (1u << (dz + 12));
           if ((w & want) != want)
             continue;
           // lowest set bit of each field: 1 - s_i; the tap a_i = 1 - s_i - d_i
-          const int lx = __ffs(w & 31u) - 1, ly = __ffs((w >> 5) & 31u) - 1,
-                    lz = __ffs((w >> 10) & 31u) - 1;
-          const int sx = 1 - lx, sy = 1 - ly, sz = 1 - lz;
-          const int ax = lx - dx, ay = ly - dy, az = lz - dz; // taps, in 0..2
-          // the children 2 p + o, fine local 2 (p local) + o
-          const double *f = sh.f + 2 * (ix + 2 + dx) + FWX * (2 * (iy + 2 + dy) +
-                                                               FWY * 2 * (iz + 2 + dz));
-          double sz_ = 0.0;
-#pragma unroll
-          for (int oz = 0; oz < 2; ++oz) {
-            double sy_ = 0.0;
-#pragma unroll
-            for (int oy = 0; oy < 2; ++oy) {
-              const double *r = f + FWX * (oy + FWY * oz);
-              const double sx_ = fma(c_eno_w[sx + 1][1][ax], r[1], c_eno_w[sx + 1][0][ax] * r[0]);
-              sy_ = fma(c_eno_w[sy + 1][oy][ay], sx_, sy_);
-            }
-            sz_ = fma(c_eno_w[sz + 1][oz][az], sy_, sz_);
-          }
-          acc += sz_;
+          const int ax = __ffs(w & 31u) - 1 - dx, ay = __ffs((w >> 5) & 31u) - 1 - dy,
+                    az = __ffs((w >> 10) & 31u) - 1 - dz;
+          acc += sh.w[(az * 3 + ay) * 3 + ax][pe];
         }
-    cbar[comp * b.cnp + (qx - b.clo[0]) + (int64_t)b.cnx * (qy - b.clo[1]) +
-         (int64_t)b.cnx * b.cny * (qz - b.clo[2])] = acc;
+    }
+    if (k == PWZ - 1) { // the component's last plane: its sums are complete
+      if (mine)
+        cbar[comp * b.cnp + (qx - b.clo[0]) + (int64_t)b.cnx * (qy - b.clo[1]) +
+             (int64_t)b.cnx * b.cny * (qz - b.clo[2])] = acc;
+      acc = 0.0;
+    }
   }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
 std::atomic<bool> g_eno_w_set[kMaxDevices];
