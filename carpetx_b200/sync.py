@@ -15,7 +15,16 @@ level's FABs, as disjoint boxes; each coarse patch is CoarseBox of its fine
 patch.  `SyncChain` builds the six plans once (per regrid) and executes them
 in order on a stream; the executions can be captured in one CUDA graph.
 With fused=True the prolongation writes the fine patches into the fine FABs
-directly and the scatter goes (five plans).
+directly and the scatter goes (five plans).  With direct=True (fused too) a
+fine patch whose coarse box lies inside one coarse FAB (ghosts included) is
+prolongated from that FAB itself, without a coarse patch; a patch that does
+not fit one FAB whole is cut at the refined faces of the coarse valid boxes
+(cell-centred directions) when every piece then fits.  The gather and the
+coarse boundary conditions remain for the other patches only.  That needs
+the coarse level's ghosts synced (its FillBoundary and boundary conditions
+done), as CarpetX's level loop has them when it fills a fine level's ghosts
+(SyncGroupsByDirI syncs the levels coarse to fine); then the FAB holds the
+values the gather and the coarse boundary conditions would give the patch.
 FABs are CUDA float64 tensors of shape (ncomp, nz, ny, nx) with inclusive
 (lo, hi) boxes and their valid boxes (valid_lo, valid_hi)."""
 import torch
@@ -54,6 +63,19 @@ def fine_patches(fabs):
     return out
 
 
+def split_at(box, cuts):
+    """Box as disjoint pieces cut before each fine index of cuts[d] inside it."""
+    pieces = [box]
+    for d in range(3):
+        out = []
+        for lo, hi in pieces:
+            xs = [c for c in cuts[d] if lo[d] < c <= hi[d]]
+            for a, b in zip([lo[d]] + xs, [x - 1 for x in xs] + [hi[d]]):
+                out.append((lo[:d] + (a,) + lo[d + 1:], hi[:d] + (b,) + hi[d + 1:]))
+        pieces = out
+    return pieces
+
+
 def _shape(lo, hi):
     return tuple(int(hi[d]) - int(lo[d]) + 1 for d in (2, 1, 0))
 
@@ -79,20 +101,58 @@ class SyncChain:
     patch of the same position, and a prolongated value depends only on its
     position and the coarse patch data, which every patch holds alike."""
 
-    def __init__(self, op, ncomp, coarse, fine, nghost, coarse_bc, fine_bc, fused=False):
+    def __init__(self, op, ncomp, coarse, fine, nghost, coarse_bc, fine_bc, fused=False,
+                 direct=False):
         dev = fine[0][0].device
-        self.fused = fused
+        fused = fused or direct
+        self.fused, self.direct = fused, direct
         self.patches = fine_patches([f[1:] for f in fine])
+
+        def holder(box):
+            """The first coarse FAB whose box holds the coarse box of a fine box."""
+            lo, hi = op.coarse_box(box[0], box[1])
+            for ci, c in enumerate(coarse):
+                if all(c[1][d] <= lo[d] and hi[d] <= c[2][d] for d in range(3)):
+                    return ci
+            return None
+
+        self.src = [None] * len(self.patches)
+        if direct:
+            # a patch read from one coarse FAB whole if it can be, else cut at
+            # the refined faces of the coarse valid boxes (cell-centred
+            # directions) if every piece then can be, else gathered whole
+            cuts = [sorted({2 * c[3][d] for c in coarse} | {2 * (c[4][d] + 1) for c in coarse})
+                    if (op.indextype >> (2 - d)) & 1 else [] for d in range(3)]
+            pats, src = [], []
+            for i, p in self.patches:
+                h = holder(p)
+                pieces, hs = [p], [h]
+                if h is None:
+                    q = split_at(p, cuts)
+                    hq = [holder(x) for x in q]
+                    if len(q) > 1 and all(x is not None for x in hq):
+                        pieces, hs = q, hq
+                pats += [(i, x) for x in pieces]
+                src += hs
+            self.patches, self.src = pats, src
         self.cpb = [op.coarse_box(p[0], p[1]) for _, p in self.patches]
-        self.cp = [torch.full((ncomp,) + _shape(lo, hi), float("nan"), dtype=torch.float64,
-                              device=dev) for lo, hi in self.cpb]
-        cpfabs = [(a, lo, hi, lo, hi) for a, (lo, hi) in zip(self.cp, self.cpb)]
+        self.cp = [None if self.src[k] is not None else
+                   torch.full((ncomp,) + _shape(lo, hi), float("nan"), dtype=torch.float64,
+                              device=dev) for k, (lo, hi) in enumerate(self.cpb)]
+        gathered = [k for k in range(len(self.cpb)) if self.src[k] is None]
+        cpfabs = [(self.cp[k], self.cpb[k][0], self.cpb[k][1], self.cpb[k][0], self.cpb[k][1])
+                  for k in gathered]
         if fused:
             self.fp = []
-            self.prolong_boxes = [
-                dict(op=op, ncomp=ncomp, crse=c, crse_lo=lo, crse_hi=hi, fine=fine[i][0],
-                     fine_lo=fine[i][1], fine_hi=fine[i][2], reg_lo=p[0], reg_hi=p[1])
-                for c, (lo, hi), (i, p) in zip(self.cp, self.cpb, self.patches)]
+            self.prolong_boxes = []
+            for k, (i, p) in enumerate(self.patches):
+                if self.src[k] is None:
+                    c, (lo, hi) = self.cp[k], self.cpb[k]
+                else:
+                    c, lo, hi = coarse[self.src[k]][:3]
+                self.prolong_boxes.append(
+                    dict(op=op, ncomp=ncomp, crse=c, crse_lo=lo, crse_hi=hi, fine=fine[i][0],
+                         fine_lo=fine[i][1], fine_hi=fine[i][2], reg_lo=p[0], reg_hi=p[1]))
         else:
             self.fp = [torch.full((ncomp,) + _shape(p[0], p[1]), float("nan"),
                                   dtype=torch.float64, device=dev) for _, p in self.patches]
@@ -100,13 +160,13 @@ class SyncChain:
                 dict(op=op, ncomp=ncomp, crse=c, crse_lo=lo, crse_hi=hi, fine=f, fine_lo=p[0],
                      fine_hi=p[1], reg_lo=p[0], reg_hi=p[1])
                 for c, (lo, hi), f, (_, p) in zip(self.cp, self.cpb, self.fp, self.patches)]
-        self.steps = [
-            ("fill_boundary", cb.CopyPlan.fill_boundary(fine, ncomp, nghost)),
-            ("gather", cb.CopyPlan.parallel_copy(cpfabs, coarse, ncomp)),
-            ("coarse_bc", cb.BoundaryPlan(coarse_bc, [(a, lo, hi) for a, (lo, hi)
-                                                      in zip(self.cp, self.cpb)])),
-            ("prolong", cb.LevelPlan(self.prolong_boxes)),
-        ]
+        self.steps = [("fill_boundary", cb.CopyPlan.fill_boundary(fine, ncomp, nghost))]
+        if cpfabs:
+            self.steps += [
+                ("gather", cb.CopyPlan.parallel_copy(cpfabs, coarse, ncomp)),
+                ("coarse_bc", cb.BoundaryPlan(coarse_bc, [f[:3] for f in cpfabs])),
+            ]
+        self.steps.append(("prolong", cb.LevelPlan(self.prolong_boxes)))
         if not fused:
             fpfabs = [(a, p[0], p[1], p[0], p[1]) for a, (_, p) in zip(self.fp, self.patches)]
             self.steps.append(("scatter", cb.CopyPlan.parallel_copy(fine, fpfabs, ncomp,

@@ -55,13 +55,17 @@ def shape(lo, hi):
     return tuple(hi[d] - lo[d] + 1 for d in (2, 1, 0))
 
 
-def level_layout():
+def level_layout(wide=False):
     """(coarse FAB boxes, fine FAB boxes, fine patches [(fab index, box)],
-    coarse patch boxes); FAB boxes as (lo, hi, valid_lo, valid_hi)."""
+    coarse patch boxes); FAB boxes as (lo, hi, valid_lo, valid_hi).  wide:
+    one fine FAB of 32 x 16 x 16 cells instead of two of 16^3, so that its
+    patches span two coarse FABs in x."""
     from region_cases import tiled
     coarse = tiled((16, 16, 16), (8, 8, 8), (1, 1, 1), NG)
     fine = []
-    for vlo, vhi in (((0, 0, 0), (15, 15, 15)), ((16, 0, 0), (31, 15, 15))):
+    valid = [((0, 0, 0), (31, 15, 15))] if wide else \
+        [((0, 0, 0), (15, 15, 15)), ((16, 0, 0), (31, 15, 15))]
+    for vlo, vhi in valid:
         fine.append((tuple(v - 3 for v in vlo), tuple(v + 3 for v in vhi), vlo, vhi))
     patches = []
     for i, (lo, hi, vlo, vhi) in enumerate(fine):
@@ -73,8 +77,8 @@ def level_layout():
     return coarse, fine, patches
 
 
-def coarse_patch_boxes(cx, patches):
-    return [cx.coarse_box(*OP, p[0], p[1]) for _, p in patches]
+def coarse_patch_boxes(cx, patches, op=OP):
+    return [cx.coarse_box(*op, p[0], p[1]) for _, p in patches]
 
 
 def specs(seed):
@@ -110,9 +114,9 @@ def initial_data(seed, coarse, fine, linear=False):
     return ca, fa
 
 
-def oracle_chain(cx, seed, linear=False):
-    coarse, fine, patches = level_layout()
-    cpb = coarse_patch_boxes(cx, patches)
+def oracle_chain(cx, seed, linear=False, op=OP, wide=False):
+    coarse, fine, patches = level_layout(wide)
+    cpb = coarse_patch_boxes(cx, patches, op)
     cs, fs = specs(seed)
     ca, fa = initial_data(seed, coarse, fine, linear)
     ffabs = [[a] + list(b) for a, b in zip(fa, fine)]
@@ -125,7 +129,7 @@ def oracle_chain(cx, seed, linear=False):
     fp = []
     for (i, (plo, phi)), f in zip(patches, cp):
         out = np.full((NCOMP,) + shape(plo, phi), np.nan)
-        cx.prolong(*OP, 0, f[0], f[1], f[2], out, plo, phi, plo, phi, NCOMP)
+        cx.prolong(*op, 0, f[0], f[1], f[2], out, plo, phi, plo, phi, NCOMP)
         fp.append([out, plo, phi, plo, phi])
     regions.parallel_copy(ffabs, fp, dst_nghost=NG)
     for f in ffabs:
