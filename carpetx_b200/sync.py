@@ -76,6 +76,36 @@ def split_at(box, cuts):
     return pieces
 
 
+def direct_sources(op, coarse, patches):
+    """The pieces of the fine patches [(fab index, box)] and, per piece, the
+    coarse FAB (index into coarse: (lo, hi, valid_lo, valid_hi) boxes) whose
+    box holds its coarse box, or None (gathered).  A patch is read from one
+    coarse FAB whole if it can be, else cut at the refined faces of the
+    coarse valid boxes (cell-centred directions) if every piece then can be,
+    else gathered whole."""
+    def holder(box):
+        lo, hi = op.coarse_box(box[0], box[1])
+        for ci, c in enumerate(coarse):
+            if all(c[0][d] <= lo[d] and hi[d] <= c[1][d] for d in range(3)):
+                return ci
+        return None
+
+    cuts = [sorted({2 * c[2][d] for c in coarse} | {2 * (c[3][d] + 1) for c in coarse})
+            if (op.indextype >> (2 - d)) & 1 else [] for d in range(3)]
+    pieces, src = [], []
+    for i, p in patches:
+        h = holder(p)
+        q, hq = [p], [h]
+        if h is None:
+            cut = split_at(p, cuts)
+            hc = [holder(x) for x in cut]
+            if len(cut) > 1 and all(x is not None for x in hc):
+                q, hq = cut, hc
+        pieces += [(i, x) for x in q]
+        src += hq
+    return pieces, src
+
+
 def _shape(lo, hi):
     return tuple(int(hi[d]) - int(lo[d]) + 1 for d in (2, 1, 0))
 
@@ -107,34 +137,9 @@ class SyncChain:
         fused = fused or direct
         self.fused, self.direct = fused, direct
         self.patches = fine_patches([f[1:] for f in fine])
-
-        def holder(box):
-            """The first coarse FAB whose box holds the coarse box of a fine box."""
-            lo, hi = op.coarse_box(box[0], box[1])
-            for ci, c in enumerate(coarse):
-                if all(c[1][d] <= lo[d] and hi[d] <= c[2][d] for d in range(3)):
-                    return ci
-            return None
-
         self.src = [None] * len(self.patches)
         if direct:
-            # a patch read from one coarse FAB whole if it can be, else cut at
-            # the refined faces of the coarse valid boxes (cell-centred
-            # directions) if every piece then can be, else gathered whole
-            cuts = [sorted({2 * c[3][d] for c in coarse} | {2 * (c[4][d] + 1) for c in coarse})
-                    if (op.indextype >> (2 - d)) & 1 else [] for d in range(3)]
-            pats, src = [], []
-            for i, p in self.patches:
-                h = holder(p)
-                pieces, hs = [p], [h]
-                if h is None:
-                    q = split_at(p, cuts)
-                    hq = [holder(x) for x in q]
-                    if len(q) > 1 and all(x is not None for x in hq):
-                        pieces, hs = q, hq
-                pats += [(i, x) for x in pieces]
-                src += hs
-            self.patches, self.src = pats, src
+            self.patches, self.src = direct_sources(op, [c[1:] for c in coarse], self.patches)
         self.cpb = [op.coarse_box(p[0], p[1]) for _, p in self.patches]
         self.cp = [None if self.src[k] is not None else
                    torch.full((ncomp,) + _shape(lo, hi), float("nan"), dtype=torch.float64,
