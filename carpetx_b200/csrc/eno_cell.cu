@@ -43,10 +43,9 @@ constexpr int EPAD = EW * EW + EW + 1;
 struct EnoShared {
   double pad0[EPAD];
   double c[EW3];    // coarse window of one component
-  double d[3][EW3]; // |undivided differences| per direction (max over the block's components)
-  double a[EW3];    // A: max over z of D_x
-  double b[EW3];    // B: max(max over z of D_y, max over y of D_z)
-  double m[EW3];    // M(p)
+  double d[3][EW3]; // |undivided differences| per direction (max over the block's
+                    // components); then, in place, A = W_z(D_x) over d[0],
+                    // B = max(W_z(D_y), W_y(D_z)) over d[1] and M over d[2]
   double p[EW3];    // the other coarse window buffer (the next item's, prefetched)
   double pad1[EPAD];
 };
@@ -85,7 +84,9 @@ struct EnoTiling {
 // (sx + 1) + 3 (sy + 1) + 9 (sz + 1), cells x fastest over t.nc; with it the
 // children are not evaluated.
 template <bool DECIDE>
-__global__ void __launch_bounds__(ENT, 2)
+// Two CTAs per SM evaluating children (124 registers); three deciding only
+// (no child evaluation: 72 registers, and the shared arrays fit three).
+__global__ void __launch_bounds__(ENT, DECIDE ? 3 : 2)
     eno_cell_kernel(const __grid_constant__ BoxDesc b, const EnoTiling t, int per_group,
                     signed char *shifts, unsigned char *fallback, unsigned char *cshift) {
   // the launches of a level's boxes after its first start in the previous
@@ -93,17 +94,16 @@ __global__ void __launch_bounds__(ENT, 2)
   // launch; no-ops without the launch attribute)
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  EnoShared &sh = *reinterpret_cast<EnoShared *>(smem_raw);
-  // the window arrays as one run of doubles, guards included, for the
+  // the window arrays (EnoShared) as one run of doubles, guards included, for the
   // neighbour reads across array ends
   double *const wbuf = reinterpret_cast<double *>(smem_raw);
   double *const C = wbuf + EPAD;
   double *const D0 = C + EW3, *const D1 = D0 + EW3, *const D2 = D1 + EW3;
-  double *const A = D2 + EW3, *const B = A + EW3, *const Mw = B + EW3;
+  double *const A = D0, *const B = D1, *const Mw = D2;
   // the coarse window alternates between c and p: while an item evaluates
   // its children, the first window of the next item is copied into the other
   // buffer with cp.async
-  double *Cc = C, *Cn = Mw + EW3;
+  double *Cc = C, *Cn = D2 + EW3;
   const int tid = threadIdx.x;
   const int rnx = b.rhi[0] - b.rlo[0] + 1, rny = b.rhi[1] - b.rlo[1] + 1;
   const int64_t rnp = (int64_t)rnx * rny * (b.rhi[2] - b.rlo[2] + 1);
@@ -198,15 +198,28 @@ __global__ void __launch_bounds__(ENT, 2)
     //      = max(W_y(A), W_x(B)),  A = W_z(D_x),  B = max(W_z(D_y), W_y(D_z)),
     // with W_a the maximum over a -1, 0, +1 along axis a (fmax is exact, so
     // the regrouping gives the same value); valid for p in [1, EW - 2]^3
+    // (three arrays in place, so that three CTAs fit an SM): W_z of D_x
+    // and D_y down each (x, y) column, the column's values held in
+    // registers; then B over D_y; then M over D_z
+    for (int tc = tid; tc < 2 * EW * EW; tc += ENT) {
+      constexpr int Z = EW * EW;
+      double *const col = (tc < Z ? D0 : D1) + tc % Z;
+      double vm = col[0], v0 = col[0]; // the ends reach no M(p) the search reads
+#pragma unroll
+      for (int k = 0; k < EW; ++k) {
+        const double vp = k + 1 < EW ? col[(k + 1) * Z] : v0;
+        col[k * Z] = fmax(fmax(vm, v0), vp);
+        vm = v0;
+        v0 = vp;
+      }
+    }
+    __syncthreads();
 #pragma unroll
     for (int n = 0; n < NWIN; ++n) {
       const int e = tid + n * ENT;
       if (e >= EW3)
         break;
-      constexpr int Z = EW * EW;
-      A[e] = fmax(fmax(D0[e - Z], D0[e]), D0[e + Z]);
-      B[e] = fmax(fmax(fmax(D1[e - Z], D1[e]), D1[e + Z]),
-                  fmax(fmax(D2[e - EW], D2[e]), D2[e + EW]));
+      B[e] = fmax(B[e], fmax(fmax(D2[e - EW], D2[e]), D2[e + EW]));
     }
     __syncthreads();
 #pragma unroll
@@ -238,7 +251,7 @@ __global__ void __launch_bounds__(ENT, 2)
             // for |s|_1 <= 3, a constant per candidate
             const int n1 = (si != 0) + (sj != 0) + (sk != 0);
             const double pen = 1.0 + 0x1p-26 * n1;
-            const double mv = sh.m[cell[q] + si + EW * sj + EW * EW * sk];
+            const double mv = Mw[cell[q] + si + EW * sj + EW * EW * sk];
             const double dd = n1 == 0 ? mv : fmul(pen, mv); // 1 * m is exact
             if (dd < min_dd) {
               min_dd = dd;
@@ -365,7 +378,7 @@ __global__ void __launch_bounds__(ENT, 2)
 
 // Per device (cache_device()): persistent grid, 0 until the kernel's dynamic
 // shared memory has been allowed on that device.
-std::atomic<int> g_eno_grid[kMaxDevices];
+std::atomic<int> g_eno_grid[kMaxDevices][2]; // [device][decisions only]
 
 } // namespace
 
@@ -392,7 +405,8 @@ cudaError_t launch_eno_cell_box(const BoxDesc &b, int per_group, signed char *sh
   if (n > INT32_MAX)
     return cudaErrorInvalidValue;
   const int dev = cache_device();
-  int grid = dev >= 0 ? g_eno_grid[dev].load() : 0;
+  const int dk = cshift ? 1 : 0;
+  int grid = dev >= 0 ? g_eno_grid[dev][dk].load() : 0;
   if (!grid) {
     cudaError_t e = cudaFuncSetAttribute(eno_cell_kernel<false>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -405,11 +419,11 @@ cudaError_t launch_eno_cell_box(const BoxDesc &b, int per_group, signed char *sh
     int per_sm = 0, d = 0, sms = 0;
     cudaGetDevice(&d);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eno_cell_kernel<false>, ENT,
-                                                  sizeof(EnoShared));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, dk ? eno_cell_kernel<true> : eno_cell_kernel<false>, ENT, sizeof(EnoShared));
     grid = sms * (per_sm > 0 ? per_sm : 1);
     if (dev >= 0)
-      g_eno_grid[dev].store(grid);
+      g_eno_grid[dev][dk].store(grid);
   }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(n < grid ? (unsigned)n : (unsigned)grid);
