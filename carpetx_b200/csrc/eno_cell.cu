@@ -481,7 +481,7 @@ struct EnoAdjShared {
 
 __constant__ double c_eno_w[3][2][3]; // [shift + 1][off][tap]
 
-__global__ void __launch_bounds__(ANT, 3)
+__global__ void __launch_bounds__(ANT, 4)
     eno_adjoint_kernel(const __grid_constant__ BoxDesc b, const EnoTiling t, int per_group,
                        const unsigned char *__restrict__ cshift, double *__restrict__ cbar,
                        int ntx, int nty) {

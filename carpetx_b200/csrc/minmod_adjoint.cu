@@ -45,14 +45,17 @@ constexpr int MNT = 256;         // threads per CTA
 enum : unsigned char { MM_ZERO = 0, MM_DM = 1, MM_DP = 2 };
 
 struct MinmodAdjShared {
-  union {
+  union { // the forward passes' arrays, then the transposed passes' (43 KB in
+           // all, so that five CTAs fit an SM)
     struct {
       double c[MCW * MCW * MCW];  // coarse window [z][y][x]
       double a1[MCW * MCW * MFW]; // A1 [cz][cy][fx]
     } fwd;
-    double g2[MT * MFW * MFW];    // Pz^T fine_bar [cz][fy][fx]
+    struct {
+      double g2[MT * MFW * MFW];  // Pz^T fine_bar [cz][fy][fx]
+      double g1[MT * MT * MFW];   // Py^T g2 [cz][cy][fx]
+    } bwd;
   } u;
-  double g1[MT * MT * MFW];       // Py^T g2 [cz][cy][fx]
   unsigned char xc[MT * MT * MCH];   // x choices [cz][cy][cx']
   unsigned char yc[MT * MCH * MFW];  // y choices [cz][cy'][fx]
   unsigned char zc[MCH * MFW * MFW]; // z choices [cz'][fy][fx]
@@ -84,7 +87,7 @@ __device__ __forceinline__ double mm_gather(const unsigned char *ch, int cs, con
   return g;
 }
 
-__global__ void __launch_bounds__(MNT, 4)
+__global__ void __launch_bounds__(MNT, 5)
     minmod_adjoint_kernel(const __grid_constant__ BoxDesc b, double *__restrict__ cbar, int ntx,
                           int nty) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -164,13 +167,13 @@ __global__ void __launch_bounds__(MNT, 4)
     const unsigned char *ch = sh.zc + i + MFW * jj;
 #pragma unroll
     for (int n = 0; n < MT; ++n)
-      sh.u.g2[i + MFW * (jj + MFW * n)] = mm_gather(ch, MFW * MFW, h, 1, n + 1);
+      sh.u.bwd.g2[i + MFW * (jj + MFW * n)] = mm_gather(ch, MFW * MFW, h, 1, n + 1);
   }
   __syncthreads();
   // 4. Py^T: g1 at (fx, cy = q0y + ny, cz = q0z + n)
   for (int e = tid; e < MFW * MT * MT; e += MNT) {
     const int i = e % MFW, ny = (e / MFW) % MT, n = e / (MFW * MT);
-    sh.g1[e] = mm_gather(sh.yc + i + MFW * MCH * n, MFW, sh.u.g2 + i + MFW * MFW * n, MFW,
+    sh.u.bwd.g1[e] = mm_gather(sh.yc + i + MFW * MCH * n, MFW, sh.u.bwd.g2 + i + MFW * MFW * n, MFW,
                          ny + 1);
   }
   __syncthreads();
@@ -180,7 +183,7 @@ __global__ void __launch_bounds__(MNT, 4)
     const int x = q0x + nx - b.clo[0], y = q0y + ny - b.clo[1], z = q0z + n - b.clo[2];
     if (x >= b.cnx || y >= b.cny || z >= cnz)
       continue;
-    const double g = mm_gather(sh.xc + MCH * (ny + MT * n), 1, sh.g1 + MFW * (ny + MT * n), 1,
+    const double g = mm_gather(sh.xc + MCH * (ny + MT * n), 1, sh.u.bwd.g1 + MFW * (ny + MT * n), 1,
                                nx + 1);
     cbar[comp * b.cnp + x + (int64_t)b.cnx * (y + (int64_t)b.cny * z)] = g;
   }
